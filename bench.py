@@ -1,0 +1,396 @@
+#!/usr/bin/env python3
+"""Benchmark of the plain-FP64 staggered phase-field fracture step on B200.
+
+A step is one staggered load increment (crack_propagation.cpp:65-121): the mechanical FAS
+multigrid solve (u_entire), the strain-history update, the phase-field FAS solve, the d
+reductions and the reaction sum, on the 257^3 three-phase inclusion/pore specimen with a
+mid-height pre-crack (seeded synthetic stand-in; every field exceeds the 126 MB L2, so no L2
+flush is needed between steps).  One process per GPU; with N > 1 each rank solves its own replica
+of the specimen (weak scaling, no data-path collective), timed on the device and reduced as the
+max over ranks.
+
+metric: MDoF-iter/s = (3 N_finest x mechanical finest-level smoother iterations
+                       + N_finest x phase-field finest-level smoother iterations) / s
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload NAME]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "MDoF-iter/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--workload", default="plain257")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-kernel-timing", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+# process group
+# ---------------------------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(tempfile.gettempdir(), f"hpc_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU reference sample (the reference's own pcg_u, compiled from its sources)
+# ---------------------------------------------------------------------------------------------
+def cpu_reference_sample(w, repeats: int = 1, nb_relax: int = 4, slab: int = 5):
+    """Times the reference's finest-level mechanical smoother pcg_u(NB_relax=nb_relax) on a
+    nx*ny*slab-node slab taken at mid-height of the workload's image, one rank (single-rank MPI
+    stand-in) with every host core as OpenMP threads.  Returns (MDoF-iter/s, info)."""
+    import numpy as np
+    from oracle import bindings as B
+    from hpcrack_b200 import microstructure as ms
+
+    nx, ny, nz = w.nodes
+    z0 = (nz - slab) // 2
+    img = np.ascontiguousarray(w.image[z0:z0 + slab])
+    enb = (nx - 1, ny - 1, slab - 1)
+    cores = os.cpu_count() or 1
+    kind = "reference" if B.RefOracle.available() else "port"
+    impl = B.RefOracle(0, enb) if kind == "reference" else B.COracle(0, enb)
+    if kind == "reference":
+        impl.set_threads(cores)
+        with tempfile.TemporaryDirectory() as td:
+            os.makedirs(os.path.join(td, "data"))
+            raw = os.path.join(td, "data", "slab.raw")
+            img.tofile(raw)
+            ms.write_material_csv(os.path.join(td, "data", "Material_Property.csv"), w.table())
+            impl.input_total(td, raw, (nx, ny, slab), w.voxel_size)
+    else:
+        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+        impl.image_material(img, (nx, ny, slab), w.table(), w.voxel_size)
+    impl.mp_choice()
+    impl.mp_all_element(w.small_k)
+    n = nx * ny * slab
+    times = []
+    for _ in range(repeats):
+        impl.set(B.U, 0, np.zeros((3, n)))
+        impl.set(B.FU, 0, np.zeros((3, n)))
+        t0 = time.perf_counter()
+        impl.pcg_u(0, w.small_k, 1.0, nb_relax, 0, 0.0)
+        times.append(time.perf_counter() - t0)
+    impl.close()
+    dt = min(times)
+    value = 3.0 * n * nb_relax / dt / 1e6
+    info = {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"pcg_u(NB_relax={nb_relax}) on the finest level of a {nx}x{ny}x{slab}-node mid-height slab "
+                      f"of the {w.name} image, 1 rank x {cores} OpenMP threads, {dt:.2f} s"}
+    return value, info
+
+
+def run_reference(args, rank, world):
+    from hpcrack_b200 import microstructure as ms
+    if rank != 0:
+        return
+    w = ms.make_workload(args.workload)
+    vals = []
+    for _ in range(max(args.warmup, 0)):
+        cpu_reference_sample(w)
+    for _ in range(args.steps):
+        v, info = cpu_reference_sample(w)
+        vals.append(v)
+    value = statistics.mean(vals)
+    info["value"] = value
+    nx, ny, nz = w.nodes
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(w, world),
+            "cpu_baseline": info,
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------------------------
+def workload_config(w, world):
+    nx, ny, nz = w.nodes
+    return {"workload": f"{w.name}: {nx}x{ny}x{nz}-node three-phase inclusion/pore specimen, pre-cracked, "
+                        f"staggered increments (mechanical + phase-field FAS V-cycles, plain FP64)",
+            "nodes": nx * ny * nz, "mech_dof": 3 * nx * ny * nz, "levels": w.maxlevel + 1,
+            "element_nb": list(w.element_nb), "mg_u": list(w.mg_u), "mg_d": list(w.mg_d),
+            "mech_tol_sq": w.mech_tol, "pf_tol_sq": w.pf_tol, "replicas": world, "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (each finest field 136 MB > 126 MB), no flush"}
+
+
+def load_specimen(w, device):
+    from hpcrack_b200 import microstructure as ms
+    from hpcrack_b200.solver import Hierarchy, H, D
+    hier = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start, device=device)
+    hier.image_material(w.image, w.nodes, w.table(), w.voxel_size)
+    if w.crack:
+        Hc, dc = ms.precrack_fields(w)
+        hier.set(H, w.maxlevel, Hc)
+        hier.set(D, w.maxlevel, dc)
+        hier.voigt_all_level(H)
+    return hier
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def run_b200(args, rank, world, local):
+    import torch
+    from hpcrack_b200 import microstructure as ms
+    from hpcrack_b200.solver import KC_MECH_PCG_FINEST, U, D, H, FU, DOLDF
+
+    torch.cuda.set_device(local)
+    w = ms.make_workload(args.workload)
+    nx, ny, nz = w.nodes
+    N = nx * ny * nz
+    hier = load_specimen(w, local)
+    stream = torch.cuda.ExternalStream(hier.stream())
+
+    def step(t):
+        return hier.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
+                         dU_factor=w.du_factor, mech_tol=w.mech_tol, pf_tol=w.pf_tol)
+
+    t = 0
+    for _ in range(args.warmup):
+        step(t)
+        t += 1
+
+    # ------------------------------------------------------------ timed region (device-resident)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    if not args.no_kernel_timing:
+        hier.kernel_timing(KC_MECH_PCG_FINEST)
+    launches0 = hier.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    outs = []
+    t_first = t
+    for _ in range(args.steps):
+        outs.append(step(t))
+        t += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    launches = hier.launch_count() - launches0
+    ms_total = e0.elapsed_time(e1)
+    kn, kms = hier.kernel_time() if not args.no_kernel_timing else (0, 0.0)
+    hier.kernel_timing(-1)
+
+    dof_iters = sum(3.0 * N * o[6] + 1.0 * N * o[7] for o in outs)
+    mech_cycles = sum(o[4] for o in outs)
+    max_ms = reduce_max(ms_total, world)
+    tot_dof_iters = reduce_sum(dof_iters, world)
+    value = tot_dof_iters / (max_ms / 1e3) / 1e6
+
+    # roofline of the dominant kernel: fused direction update + K(d) p + (p, w) on the finest level.
+    # Algorithmic bytes per finest node: r, preM, p_old, p_new, w (3 x 8 B each), bulK, G, d (8 B each),
+    # regime (1 B) = 145 B; the first iteration of each smoother call does not read p_old (121 B).
+    roofline = None
+    if kn > 0:
+        firsts = 2 * mech_cycles if w.maxlevel >= 1 else mech_cycles
+        firsts = min(firsts, kn)
+        bytes_total = N * (145.0 * (kn - firsts) + 121.0 * firsts)
+        achieved = bytes_total / (kms / 1e3) / 1e9
+        peak, src = peaks()
+        roofline = {"bound": "hbm", "kernel": "mech_kernel<finest, PCG> (fused z/p update + K(d)p + pw)",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_source": src, "traffic": None, "launches": kn, "avg_launch_ms": kms / kn,
+                    "bytes_per_node": [145, 121]}
+
+    # ------------------------------------------------------------ end to end through the C ABI
+    e2e = None
+    if not args.no_e2e:
+        Lf = w.maxlevel
+        pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True)  # noqa: E731
+        hu, hfu = pin(3 * N), pin(3 * N)
+        hd, hH, hdo = pin(N), pin(N), pin(N)
+        # start from the current state, held on the host
+        dptr = lambda ten: C.cast(ten.data_ptr(), C.POINTER(C.c_double))  # noqa: E731
+        lib = hier.lib
+
+        def down(field, ten, ncomp):
+            for c in range(ncomp):
+                lib.hpc_download(hier.h, field, Lf, c, C.cast(ten.data_ptr() + 8 * c * N, C.POINTER(C.c_double)))
+
+        def up(field, ten, ncomp):
+            for c in range(ncomp):
+                lib.hpc_upload(hier.h, field, Lf, c, C.cast(ten.data_ptr() + 8 * c * N, C.POINTER(C.c_double)))
+
+        down(U, hu, 3); down(FU, hfu, 3); down(D, hd, 1); down(H, hH, 1); down(DOLDF, hdo, 1)
+        barrier(world)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        e2e_iters = 0.0
+        for _ in range(args.steps):
+            up(U, hu, 3); up(FU, hfu, 3); up(D, hd, 1); up(H, hH, 1); up(DOLDF, hdo, 1)
+            o = step(t)
+            t += 1
+            down(U, hu, 3); down(FU, hfu, 3); down(D, hd, 1); down(H, hH, 1)
+            e2e_iters += 3.0 * N * o[6] + 1.0 * N * o[7]
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        e2e_ms = reduce_max(f0.elapsed_time(f1), world)
+        e2e_val = reduce_sum(e2e_iters, world) / (e2e_ms / 1e3) / 1e6
+        e2e = {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": 8 * N * 9, "d2h_bytes_per_step": 8 * N * 8,
+               "ms_per_step": e2e_ms / args.steps}
+        del hu, hfu, hd, hH, hdo
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            _, cpu = cpu_reference_sample(w)
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "unavailable",
+                   "sample": f"failed: {exc}"}
+
+    hier.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": workload_config(w, world), "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roofline, "cpu_baseline": cpu,
+                "solves_per_s": world * args.steps / (max_ms / 1e3),
+                "steps_detail": [{"t": t_first + i, "mech_cycles": int(o[4]), "pf_cycles": int(o[5]),
+                                  "mech_iters": int(o[6]), "pf_iters": int(o[7]), "F": o[1], "dmax": o[3]}
+                                 for i, o in enumerate(outs)]}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_b200(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,199 @@
+// Internal declarations of the B200 HPCrack library: context, level descriptors and kernel
+// launchers.  Host code is C++17; device code is CUDA for sm_100a.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+
+#include "../../include/hpcrack.h"
+
+namespace hpc {
+
+constexpr int kMaxLevels = 16;
+constexpr int kPitchAlign = 4;  // x pitch rounded to 4 doubles (32 B): 16-byte aligned rows
+
+// Geometry of one level as the kernels see it.  Arrays are x-fastest with an x pitch `px` >= nx;
+// padding slots are kept at zero in every vector (and at one in diagonals) so flat vector kernels
+// may run over the padded range.
+struct LevelGeo {
+  int nx, ny, nz, px;
+  long long plane;  // px * ny
+  long long n;      // px * ny * nz (padded slots)
+  double hx, hy, hz, wg;
+  // Dirichlet node sets, selected by floating-point coordinate equality exactly as
+  // boundary_conditions.cpp:20-68 does; they are separable per axis:
+  //   bx[i] bit0: x == (xa+xb)/2   bit1: x == xb
+  //   by[j] bit0: y == ya          bit1: y == (ya+yb)/2
+  //   bz[k] bit0: z == za          bit1: z == zb
+  const uint8_t* bx;
+  const uint8_t* by;
+  const uint8_t* bz;
+};
+
+struct LevelFields {
+  double *bulK, *G, *gc, *d, *H, *fd, *Ke, *Ge, *R, *dold;
+  double *u, *fu, *ru, *uold;  // 3n each; component c at +c*n
+  int8_t* choice;
+  // work arrays
+  double *preMu, *p, *w, *tmp3;  // 3n
+  double *preMd, *pd, *wd, *tmp1;  // n
+  uint8_t* bc_host_copy;           // host copies of the axis flags (nx+ny+nz bytes)
+};
+
+// Device scalar pool layout (doubles).
+enum Scalar : int {
+  S_FNORM = 0,    // f_norm of the mechanical solve (pcg_u at t == 0, finest)
+  S_FDNORM = 1,   // fd_norm (rewritten by every pcg_d)
+  S_RNORM = 2,    // last squared residual norm
+  S_RES0 = 3,     // generic reduction results
+  S_RES1 = 4,
+  S_RES2 = 5,
+  S_PCG = 16,     // pcg scratch: rz[-1..kMaxRelax], pw[0..kMaxRelax), rn[0..kMaxRelax)
+};
+constexpr int kMaxRelax = 4096;
+constexpr int S_ZEROS = S_PCG + 3 * (kMaxRelax + 2);  // zero-diagonal counts, one slot per level
+constexpr int kScalarPool = S_ZEROS + 16;
+inline int slot_rz(int it) { return S_PCG + 1 + it; }  // it >= -1
+inline int slot_pw(int it) { return S_PCG + (kMaxRelax + 2) + it; }
+inline int slot_rn(int it) { return S_PCG + 2 * (kMaxRelax + 2) + it; }
+
+}  // namespace hpc
+
+struct hpc_ctx {
+  hpc_geometry geo;
+  int maxlevel;
+  double box[6];  // xa xb ya yb za zb
+  hpc::LevelGeo L[hpc::kMaxLevels];
+  hpc::LevelFields F[hpc::kMaxLevels];
+  double* d_old;  // finest d of the previous increment
+  cudaStream_t stream;
+  int device;
+  double* scal;          // device scalar pool
+  double* hscal;         // pinned host staging for scalar reads
+  double* partials;      // per-block reduction partials
+  unsigned int* counter; // last-block-done counter
+  size_t partials_cap;   // doubles
+  void* bc_dev_base;     // one allocation for all axis flags
+  long long launches;
+  int choice_quirk;
+  // per-class launch timing (hpc_kernel_timing)
+  int timing_class;
+  cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
+  int tev_cap, tev_used;
+  double f_norm, fd_norm, Ue, Ut, dU, uprop;  // staggered-loop state (crack_propagation.cpp:32-39)
+};
+
+namespace hpc {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+int cuda_fail(cudaError_t e, const char* where);
+#define HPC_CUDA(call)                                            \
+  do {                                                            \
+    cudaError_t _e = (call);                                      \
+    if (_e != cudaSuccess) return ::hpc::cuda_fail(_e, #call);    \
+  } while (0)
+#define HPC_CHECK_LAUNCH(ctx)                                               \
+  do {                                                                      \
+    (ctx)->launches++;                                                      \
+    cudaError_t _e = cudaGetLastError();                                    \
+    if (_e != cudaSuccess) return ::hpc::cuda_fail(_e, "kernel launch");    \
+  } while (0)
+
+// Launch timing: bracket a launch of class `cls` with events when that class is being timed.
+void timing_begin(hpc_ctx* c, int cls);
+void timing_end(hpc_ctx* c, int cls);
+
+// ---------------------------------------------------------------- field access
+double* scalar_field(hpc_ctx* c, int field, int level);  // nullptr if not a scalar field
+double* vector_field(hpc_ctx* c, int field, int level);  // nullptr if not a vector field
+int read_scalars(hpc_ctx* c, int first, int count, double* out);  // sync + D2H of scalar slots
+int write_scalar(hpc_ctx* c, int slot, double v);
+
+// ---------------------------------------------------------------- kernel launchers (kernels.cu)
+// Element operators.  `src` is a 3n (mech) or n (pf) vector on level L.
+enum MechEpi { EPI_PLAIN = 0, EPI_RESIDUAL = 1, EPI_PCG = 2, EPI_FAS = 3, EPI_REACTION = 4 };
+
+struct MechCall {
+  int level;
+  bool finest;
+  int epi;
+  const double* src;  // u (PLAIN / RESIDUAL / FAS / REACTION) or p_old (PCG)
+  double* out;        // Fi (PLAIN), r (RESIDUAL), w (PCG), fc (FAS), fu (REACTION: BC slots only)
+  double small_k;
+  // RESIDUAL: r = fu - K u, zero at Dirichlet nodes; optionally fu[bc] = (K u)[bc] and f_norm.
+  double* fu;
+  bool set_fnorm;     // t == 0 on the finest level (mechanical_pcg.cpp:252-258)
+  const double* preM; // RESIDUAL: rz = sum r^2/preM ; PCG: z = r/preM
+  // PCG: p_new = r/preM + beta p_old with beta = scal[s_rz]/scal[s_rz_prev] (0 if first)
+  const double* r;
+  double* p_new;
+  int s_rz, s_rz_prev, first;
+  // FAS: fc = K_c u_c + full-weighting(rf)
+  const double* rf;
+  int fine_level;
+  // reduction destinations (scalar slots, -1 = none)
+  int s_out0, s_out1, s_out2;
+};
+int launch_mech(hpc_ctx* c, const MechCall& m);
+int launch_mech_diag(hpc_ctx* c, int level, bool finest, double small_k, double* out);
+
+struct PfCall {
+  int level;
+  int epi;  // EPI_PLAIN, EPI_RESIDUAL, EPI_PCG, EPI_FAS
+  const double* src;
+  double* out;
+  double lc;
+  const double* fd;     // RESIDUAL: R = fd - A d
+  const double* preM;   // PCG
+  const double* r;
+  double* p_new;
+  int s_rz, s_rz_prev, first;
+  const double* rf;
+  int fine_level;
+  int s_out0, s_out1, s_out2;
+};
+int launch_pf(hpc_ctx* c, const PfCall& p);
+int launch_pf_diag(hpc_ctx* c, int level, double lc, double* out);
+
+// Vector kernels.
+// Mechanical CG update: alpha = scal[s_rz]/scal[s_pw]; u += alpha p; r -= alpha w; r = 0 on Dirichlet
+// nodes; scal[s_rz_next] = sum r^2/preM; scal[s_rn] = sum r^2.
+int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
+int launch_pf_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
+// Dirichlet operations on a 3n vector of a level: kind 0 set u (Ut on top), 1 copy src into v,
+// 2 zero v.
+int launch_bc(hpc_ctx* c, int level, double* v, const double* src, int kind, double Ut);
+// sum of squares of a 3n (ncomp=3) or n vector into scal[slot]; optional second vector for dots.
+int launch_dot(hpc_ctx* c, int level, int ncomp, const double* a, const double* b, int slot);
+// fill / copy helpers over padded levels
+int launch_fill(hpc_ctx* c, double* v, long long n, double value);
+int launch_axpby(hpc_ctx* c, double* y, const double* a, const double* b, double sa, double sb, long long n);
+// Transfers
+int launch_inject(hpc_ctx* c, int lf, const double* f, double* co, int ncomp);
+int launch_inject_u(hpc_ctx* c, int lf, double Ut);  // u_c = u_f(2i), BC, uold_c = u_c (coarsen_u)
+int launch_inject_d(hpc_ctx* c, int lf);             // d_c = d_f(2i), dold_c = d_c (coarsen_d)
+int launch_restrict(hpc_ctx* c, int lf, const double* rf, const double* Fic, double* fc, int ncomp);
+int launch_prolong(hpc_ctx* c, int lf, const double* uc, const double* ucold, double* uf, int ncomp,
+                   bool apply_bc, double Ut);
+// Material / history
+int launch_choice_element(hpc_ctx* c, double small_k, bool do_choice, bool do_element);
+int launch_vr(hpc_ctx* c, int lf, const double* Hf, double* Hc, bool hill, bool whole_array);
+int launch_coarse_vr(hpc_ctx* c, int lf, const double* f, double* co);
+int launch_strain_history(hpc_ctx* c, double lc, double uprop);
+int launch_fd_h(hpc_ctx* c, int level);
+int launch_dmax(hpc_ctx* c, int slot_dd, int slot_dmax, bool copy_old);
+int launch_ue(hpc_ctx* c, double lc, int slot);
+int launch_top_sum(hpc_ctx* c, int slot);
+int launch_initial_crack(hpc_ctx* c, int level, double H_crack);
+int launch_image_material(hpc_ctx* c, const uint8_t* dimage, const int* voxel_n, int ngray, const int* dgray,
+                          const double* dE, const double* dnu, const double* dgc, double voxel_size);
+int launch_mp_choice_level(hpc_ctx* c, int level);
+int launch_choice_level(hpc_ctx* c, int level, double small_k, bool do_choice, bool do_element);
+int launch_crack(hpc_ctx* c, int level, const uint8_t* fx, const uint8_t* fy, const uint8_t* fz, double Hc);
+int launch_zero_count(hpc_ctx* c, int level, int ncomp, const double* v, int slot);
+int upload_shape_table(const double* N64);
+
+}  // namespace hpc

@@ -1,0 +1,297 @@
+"""Host-side mirror of HPCrack's solver interface over the B200 library.
+
+:class:`Hierarchy` owns one device context (the mg / mgvec containers of the
+reference: crack_propagation.cpp:40-45) and exposes the reference's operations
+under their own names - ``internal_force`` (Internal_Force), ``pcg_u``,
+``cycle_u``, ``u_entire``, ``fld``, ``pcg_d``, ``cycle_d``, ``phase_field``,
+``strain_history``, ``fd_h``, ``delta_d_max``, ... - with the same argument
+meaning.  Arrays cross the boundary in the reference's layout: x-fastest
+nx*ny*nz doubles per level, vector fields as (3, n).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import lib as _L
+
+# field ids (include/hpcrack.h enum hpc_field)
+BULK, G, GC, D, H, FD, KE, GE, R, DOLD, DOLDF = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10
+U, FU, RU, UOLD = 16, 17, 18, 19
+VECTOR_FIELDS = (U, FU, RU, UOLD)
+KC_MECH_PCG_FINEST, KC_PF_PCG_FINEST, KC_MECH_UPDATE_FINEST = 0, 1, 2
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def mg_params(mg5) -> _L.hpc_mg:
+    """(nu0, nu1, nu2, gamma, ncy) -> hpc_mg (the reference's MG struct, mg.h:18-25)."""
+    return _L.hpc_mg(*[int(v) for v in mg5])
+
+
+class Hierarchy:
+    """Device-resident multigrid hierarchy of one specimen."""
+
+    def __init__(self, maxlevel, enb, x0=(0.0, 0.0, 0.0), roi=(0, 0, 0), device: int = 0):
+        self.lib = _L.load()
+        self.maxlevel = int(maxlevel)
+        self.enb = tuple(int(e) for e in enb)
+        self.geo = _L.hpc_geometry(self.maxlevel, (C.c_int * 3)(*self.enb), (C.c_double * 3)(*map(float, x0)),
+                                   (C.c_int * 3)(*map(int, roi)))
+        h = C.c_void_p()
+        _L.check("hpc_create", self.lib.hpc_create(C.byref(h), C.byref(self.geo), int(device)))
+        self.h = h
+        self.dims = [tuple(e * (1 << l) + 1 for e in self.enb) for l in range(self.maxlevel + 1)]
+
+    # ------------------------------------------------------------ lifetime
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hpc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def footprint(maxlevel, enb, x0=(0.0, 0.0, 0.0), roi=(0, 0, 0)) -> int:
+        lib = _L.load()
+        geo = _L.hpc_geometry(int(maxlevel), (C.c_int * 3)(*map(int, enb)), (C.c_double * 3)(*map(float, x0)),
+                              (C.c_int * 3)(*map(int, roi)))
+        out = C.c_size_t(0)
+        _L.check("hpc_footprint", lib.hpc_footprint(C.byref(geo), C.byref(out)))
+        return out.value
+
+    def _c(self, name, *args):
+        _L.check(name, getattr(self.lib, name)(self.h, *args))
+
+    # ------------------------------------------------------------ fields
+    def n(self, level):
+        d = self.dims[level]
+        return d[0] * d[1] * d[2]
+
+    def level_dims(self, level):
+        n3 = (C.c_int * 3)()
+        h3 = (C.c_double * 3)()
+        self._c("hpc_level_dims", level, n3, h3)
+        return tuple(n3), tuple(h3)
+
+    def set(self, field, level, arr):
+        nn = self.n(level)
+        if field in VECTOR_FIELDS:
+            a = np.ascontiguousarray(arr, dtype=np.float64).reshape(3, nn)
+            for c in range(3):
+                row = np.ascontiguousarray(a[c])
+                self._c("hpc_upload", field, level, c, _dptr(row))
+        else:
+            a = np.ascontiguousarray(arr, dtype=np.float64).reshape(nn)
+            self._c("hpc_upload", field, level, 0, _dptr(a))
+
+    def get(self, field, level):
+        nn = self.n(level)
+        if field in VECTOR_FIELDS:
+            out = np.empty((3, nn))
+            for c in range(3):
+                row = np.empty(nn)
+                self._c("hpc_download", field, level, c, _dptr(row))
+                out[c] = row
+            return out
+        out = np.empty(nn)
+        self._c("hpc_download", field, level, 0, _dptr(out))
+        return out
+
+    def set_choice(self, level, arr):
+        a = np.ascontiguousarray(arr, dtype=np.int16).reshape(self.n(level))
+        self._c("hpc_upload_choice", level, a.ctypes.data_as(C.POINTER(C.c_int16)))
+
+    def get_choice(self, level):
+        a = np.empty(self.n(level), dtype=np.int16)
+        self._c("hpc_download_choice", level, a.ctypes.data_as(C.POINTER(C.c_int16)))
+        return a
+
+    def set_choice_quirk(self, reproduce: bool):
+        self._c("hpc_set_choice_quirk", int(bool(reproduce)))
+
+    def state(self):
+        s = (C.c_double * 6)()
+        self._c("hpc_get_state", s)
+        return list(s)
+
+    def set_state(self, s6):
+        self._c("hpc_set_state", (C.c_double * 6)(*s6))
+
+    def launch_count(self, reset=False) -> int:
+        v = C.c_longlong(0)
+        self._c("hpc_launch_count", C.byref(v), int(reset))
+        return v.value
+
+    def sync(self):
+        self._c("hpc_sync")
+
+    def stream(self) -> int:
+        return self.lib.hpc_stream(self.h) or 0
+
+    def kernel_timing(self, kernel_class: int):
+        """Start recording CUDA-event durations of every launch of `kernel_class` (-1 stops)."""
+        self._c("hpc_kernel_timing", int(kernel_class))
+
+    def kernel_time(self):
+        """(launches, total device ms) recorded since kernel_timing()."""
+        n = C.c_longlong(0)
+        ms = C.c_double(0)
+        self._c("hpc_kernel_time", C.byref(n), C.byref(ms))
+        return n.value, ms.value
+
+    # ------------------------------------------------------------ operators
+    def internal_force(self, level, src, dst, small_k):
+        self._c("hpc_internal_force", level, src, dst, small_k)
+
+    def prem_u(self, level, dst, small_k):
+        self._c("hpc_prem_u", level, dst, small_k)
+
+    def fld(self, level, src, dst, lc):
+        self._c("hpc_fld", level, src, dst, lc)
+
+    def precondition_m(self, level, dst, lc):
+        self._c("hpc_precondition_m", level, dst, lc)
+
+    # ------------------------------------------------------------ smoothers / solves
+    def initial_residual_u(self, level, small_k):
+        r = C.c_double(0)
+        self._c("hpc_initial_residual_u", level, small_k, C.byref(r))
+        return r.value
+
+    def pcg_u(self, level, small_k, Ut, nb_relax, t, f_norm):
+        fn = C.c_double(f_norm)
+        self._c("hpc_pcg_u", level, small_k, Ut, nb_relax, t, C.byref(fn))
+        return nb_relax, fn.value
+
+    def initial_residual_d(self, level, lc):
+        r = C.c_double(0)
+        self._c("hpc_initial_residual_d", level, lc, C.byref(r))
+        return r.value
+
+    def pcg_d(self, level, lc, nb_relax, t, fd_norm):
+        fn = C.c_double(fd_norm)
+        self._c("hpc_pcg_d", level, lc, nb_relax, t, C.byref(fn))
+        return nb_relax, fn.value
+
+    def cycle_u(self, level, mg5, small_k, Ut, t, f_norm):
+        fn = C.c_double(f_norm)
+        mg = mg_params(mg5)
+        self._c("hpc_cycle_u", level, C.byref(mg), small_k, Ut, t, C.byref(fn))
+        return None, fn.value
+
+    def cycle_d(self, level, mg5, lc, t, fd_norm):
+        fn = C.c_double(fd_norm)
+        mg = mg_params(mg5)
+        self._c("hpc_cycle_d", level, C.byref(mg), lc, t, C.byref(fn))
+        return None, fn.value
+
+    def u_entire(self, mg5, small_k, Ut, t, f_norm, mech_tol=1e-6):
+        fn = C.c_double(f_norm)
+        cy, it = C.c_int(0), C.c_int(0)
+        mg = mg_params(mg5)
+        self._c("hpc_u_entire", C.byref(mg), small_k, Ut, t, C.byref(fn), mech_tol, C.byref(cy), C.byref(it))
+        return cy.value, it.value, fn.value
+
+    def phase_field(self, mg5, lc, t, fd_norm, pf_tol=1e-12):
+        fn = C.c_double(fd_norm)
+        cy, it = C.c_int(0), C.c_int(0)
+        mg = mg_params(mg5)
+        self._c("hpc_phase_field", C.byref(mg), lc, t, C.byref(fn), pf_tol, C.byref(cy), C.byref(it))
+        return cy.value, it.value, fn.value
+
+    def step(self, t, mg_u, mg_d, small_k, lc, voxel_size, ut0=0.0, dU=0.0, dU_factor=1.5e-3, mech_tol=1e-6,
+             pf_tol=1e-12):
+        p = _L.hpc_step_params(int(t), mg_params(mg_u), mg_params(mg_d), small_k, lc, voxel_size, ut0, dU, dU_factor,
+                               mech_tol, pf_tol)
+        out = (C.c_double * 8)()
+        self._c("hpc_step", C.byref(p), out)
+        return list(out)
+
+    # ------------------------------------------------------------ material / history
+    def mp_choice(self):
+        self._c("hpc_mp_choice")
+
+    def mp_all_element(self, small_k):
+        self._c("hpc_mp_all_element", small_k)
+
+    def vr_all_level(self, field):
+        self._c("hpc_vr_all_level", field)
+
+    def voigt_all_level(self, field):
+        self._c("hpc_voigt_all_level", field)
+
+    def coarse_vr(self, field):
+        self._c("hpc_coarse_vr", field)
+
+    def strain_history(self, lc, u_proportion):
+        self._c("hpc_strain_history", lc, u_proportion)
+
+    def fd_h(self, level):
+        self._c("hpc_fd_h", level)
+
+    def _scalar(self, name, *args):
+        v = C.c_double(0)
+        self._c(name, *args, C.byref(v))
+        return v.value
+
+    def delta_d_max(self):
+        return self._scalar("hpc_delta_d_max")
+
+    def d_max(self):
+        return self._scalar("hpc_d_max")
+
+    def U_e(self, lc):
+        return self._scalar("hpc_U_e", lc)
+
+    def externe_force_nodal(self, Ut, small_k):
+        self._c("hpc_externe_force_nodal", Ut, small_k)
+
+    def externe_force_sum(self):
+        return self._scalar("hpc_externe_force_sum")
+
+    def initial_crack(self, H_crack, level):
+        self._c("hpc_initial_crack", H_crack, level)
+
+    # ------------------------------------------------------------ boundary conditions / transfers
+    def dirichlet_bd(self, level, field, Ut):
+        self._c("hpc_dirichlet_bd", level, field, Ut)
+
+    def dirichlet_force(self, level, f_field, fi_field):
+        self._c("hpc_dirichlet_force", level, f_field, fi_field)
+
+    def dirichlet_residual(self, level, field):
+        self._c("hpc_dirichlet_residual", level, field)
+
+    def solution_injection(self, field, comp, lf):
+        self._c("hpc_solution_injection", field, comp, lf)
+
+    def coarsen_f_standard(self, fc_field, rf_field, fic_field, comp, lf):
+        self._c("hpc_coarsen_f_standard", fc_field, rf_field, fic_field, comp, lf)
+
+    def refine_standard(self, uf_field, uc_field, ucold_field, comp, lf):
+        self._c("hpc_refine_standard", uf_field, uc_field, ucold_field, comp, lf)
+
+    # ------------------------------------------------------------ input path
+    def image_material(self, image, voxel_n, table, voxel_size):
+        gray, E, nu, gcv = table
+        img = np.ascontiguousarray(image, dtype=np.uint8).ravel()
+        g = np.ascontiguousarray(gray, dtype=np.int32)
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        nu = np.ascontiguousarray(nu, dtype=np.float64)
+        gcv = np.ascontiguousarray(gcv, dtype=np.float64)
+        self._c("hpc_image_material", img.ctypes.data_as(C.POINTER(C.c_uint8)), (C.c_int * 3)(*map(int, voxel_n)),
+                len(g), g.ctypes.data_as(C.POINTER(C.c_int)), _dptr(E), _dptr(nu), _dptr(gcv), voxel_size)

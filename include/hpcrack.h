@@ -1,0 +1,218 @@
+/*
+ * hpcrack.h - C ABI of the B200 library for HPCrack's staggered phase-field
+ * fracture hot path (matrix-free FAS multigrid with restarted Jacobi-PCG
+ * smoothers on trilinear-hex voxel grids).
+ *
+ * Every entry point returns an int status (HPC_OK = 0, see hpc_status); a
+ * failing call leaves a message readable with hpc_last_error().  No entry point
+ * falls back to the CPU: without a usable CUDA device hpc_create fails.
+ *
+ * Data layout seen by the caller is the reference's (include/grid.h:83-91):
+ * one level of one field is a dense nx*ny*nz array of doubles, x fastest;
+ * element (i,j,k) data live at node (i,j,k) of a node-sized array; level 0 is
+ * the coarsest (include/mg.h:54-65).  Vector fields (u, fu, ru, uold) have
+ * three components addressed by `comp`.  The library keeps device mirrors of
+ * the whole hierarchy (gridded with an x pitch rounded up to 4 doubles) and
+ * converts on hpc_upload / hpc_download.
+ *
+ * The reference has no FFI of its own: its interface is the set of C++ free
+ * functions over grid<T>& / gdvec<T>& / mg<T>& declared in include/*.h of the
+ * HPCrack project.  Each entry point below names the reference function it
+ * replaces (path:line in the HPCrack project); the C++ drop-in shims in
+ * hpcrack_b200/shim/ keep those exact signatures and call these functions.
+ *
+ * Threading: one host thread per context; all work of a context runs in order
+ * on that context's CUDA stream.
+ */
+#ifndef HPCRACK_B200_H
+#define HPCRACK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hpc_ctx hpc_ctx;
+
+enum hpc_status {
+  HPC_OK = 0,
+  HPC_ERR_ARG = 1,        /* bad argument (level, field, size, null pointer) */
+  HPC_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+  HPC_ERR_NOMEM = 3,      /* device allocation refused */
+  HPC_ERR_DIVZERO = 4,    /* zero diagonal entry: the reference throws "Division by zero in grid /=
+                             operation" (include/grid.h:182-190) */
+  HPC_ERR_INPUT = 5,      /* gray level outside the material table, malformed input */
+  HPC_ERR_NODEVICE = 6    /* no CUDA device */
+};
+
+/* Field ids (the reference's containers: crack_propagation.cpp:40-45, mechanical_displacement.cpp:
+ * 28-35, phase_field.cpp:19-20). */
+enum hpc_field {
+  HPC_BULK = 0,   /* bulk modulus K, nodal, every level */
+  HPC_G = 1,      /* shear modulus G, nodal */
+  HPC_GC = 2,     /* fracture toughness Gc, nodal */
+  HPC_D = 3,      /* phase field d */
+  HPC_H = 4,      /* strain-history field H, element */
+  HPC_FD = 5,     /* phase-field right-hand side */
+  HPC_KE = 6,     /* element bulk modulus K_element */
+  HPC_GE = 7,     /* element shear modulus G_element */
+  HPC_R = 8,      /* phase-field residual */
+  HPC_DOLD = 9,   /* coarse-level d saved at injection */
+  HPC_DOLDF = 10, /* finest d of the previous increment (d_old) */
+  HPC_U = 16,     /* displacement, 3 components */
+  HPC_FU = 17,    /* mechanical right-hand side / reactions */
+  HPC_RU = 18,    /* mechanical residual */
+  HPC_UOLD = 19,  /* coarse-level u saved at injection */
+  HPC_CHOICE = 32 /* regime 0/1/2 per element (int16 on the host side) */
+};
+
+typedef struct {
+  int maxlevel;          /* finest level index; level 0 is the coarsest */
+  int element_nb[3];     /* elements per axis on the coarsest level (config element_nb) */
+  double x_start[3];     /* domain origin (config X_start) */
+  int roi_start[3];      /* image ROI start (config ROI_start_*) */
+} hpc_geometry;
+
+/* Multigrid parameters, the reference's MG struct (include/mg.h:18-25). */
+typedef struct {
+  int nu0, nu1, nu2, gamma, ncy;
+} hpc_mg;
+
+/* One staggered load increment (crack_propagation.cpp:65-121) with its constants as parameters. */
+typedef struct {
+  int t;               /* increment index; t == 0 sets f_norm from reactions and Ue */
+  hpc_mg mg_u, mg_d;
+  double small_k;      /* residual stiffness k (crack_propagation.cpp:32) */
+  double lc;           /* phase-field length scale l (already multiplied by h, main.cpp:94) */
+  double voxel_size;   /* reaction scaling (crack_propagation.cpp:96) */
+  double ut0;          /* <= 0: Ut0 = Ue (U_e) and dU = du_factor * Ue, as the reference */
+  double du;           /* load step when ut0 > 0 */
+  double du_factor;    /* 1.5e-3 in the reference (crack_propagation.cpp:76) */
+  double mech_tol;     /* squared ratio |r|^2/|f|^2 (1e-6 in mechanical_displacement.cpp:88) */
+  double pf_tol;       /* squared tests of phase_field.cpp:30-43 (1e-12 there) */
+} hpc_step_params;
+
+/* ---------------- context ---------------- */
+
+/* Allocates the device mirrors of the whole hierarchy on `device`. */
+int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device);
+int hpc_destroy(hpc_ctx* ctx);
+/* Device bytes hpc_create would allocate for this geometry (admission by HBM footprint). */
+int hpc_footprint(const hpc_geometry* geo, size_t* bytes);
+/* Level geometry as initialize() builds it (initialization.cpp:19-134). */
+int hpc_level_dims(hpc_ctx* ctx, int level, int* n3, double* h3);
+int hpc_sync(hpc_ctx* ctx);
+const char* hpc_last_error(void);
+/* 1 (default) reproduces the reference's MP_choice loop bounds (material_selection.cpp:60-63),
+ * 0 visits every element. */
+int hpc_set_choice_quirk(hpc_ctx* ctx, int reproduce);
+/* Kernels launched by this context since the last reset (instrumentation for benchmarks). */
+int hpc_launch_count(hpc_ctx* ctx, long long* count, int reset);
+/* The context's CUDA stream (cudaStream_t), for callers that time on it. */
+void* hpc_stream(hpc_ctx* ctx);
+/* Kernel classes that can be timed with CUDA events on the context's stream. */
+enum hpc_kernel_class {
+  HPC_KC_NONE = -1,
+  HPC_KC_MECH_PCG_FINEST = 0,   /* fused direction update + K(d) p + (p, w) on the finest level */
+  HPC_KC_PF_PCG_FINEST = 1,     /* fused direction update + A_d p + (p, w) on the finest level */
+  HPC_KC_MECH_UPDATE_FINEST = 2 /* u += alpha p, r -= alpha w, rz and |r|^2 on the finest level */
+};
+/* Records a start/stop event pair around every launch of `kernel_class` from now on (HPC_KC_NONE
+ * stops recording); resets the record. */
+int hpc_kernel_timing(hpc_ctx* ctx, int kernel_class);
+/* Synchronises and returns the number of recorded launches and their summed device time (ms). */
+int hpc_kernel_time(hpc_ctx* ctx, long long* launches, double* total_ms);
+
+/* ---------------- host <-> device (dense x-fastest host arrays) ---------------- */
+int hpc_upload(hpc_ctx* ctx, int field, int level, int comp, const double* host);
+int hpc_download(hpc_ctx* ctx, int field, int level, int comp, double* host);
+int hpc_upload_choice(hpc_ctx* ctx, int level, const int16_t* host);
+int hpc_download_choice(hpc_ctx* ctx, int level, int16_t* host);
+/* Loop state of the staggered driver: {f_norm, fd_norm, Ue, Ut, dU, u_proportion}. */
+int hpc_get_state(hpc_ctx* ctx, double* s6);
+int hpc_set_state(hpc_ctx* ctx, const double* s6);
+
+/* ---------------- operators ---------------- */
+/* Internal_Force: dst = K(d) src on one level (mechanical_pcg.cpp:174-191). */
+int hpc_internal_force(hpc_ctx* ctx, int level, int src_field, int dst_field, double small_k);
+/* PreM_u: dst = diag K(d) (mechanical_pcg.cpp:102-112). */
+int hpc_prem_u(hpc_ctx* ctx, int level, int dst_field, double small_k);
+/* Fld: dst = A_d src (phase_field_pcg.cpp:93-103). */
+int hpc_fld(hpc_ctx* ctx, int level, int src_field, int dst_field, double lc);
+/* Precondition_M: dst = diag A_d (phase_field_pcg.cpp:49-59). */
+int hpc_precondition_m(hpc_ctx* ctx, int level, int dst_field, double lc);
+
+/* ---------------- smoothers, cycles, solves ---------------- */
+/* Initial_residual_u (mechanical_pcg.cpp:193-220). */
+int hpc_initial_residual_u(hpc_ctx* ctx, int level, double small_k, double* r_norm);
+/* pcg_u (mechanical_pcg.cpp:223-330; declared mechanical_pcg.h:47-51). */
+int hpc_pcg_u(hpc_ctx* ctx, int level, double small_k, double Ut, int nb_relax, int t, double* f_norm);
+/* initial_residual (phase_field_pcg.cpp:106-131). */
+int hpc_initial_residual_d(hpc_ctx* ctx, int level, double lc, double* r_norm);
+/* pcg_d (phase_field_pcg.cpp:133-214; declared phase_field_pcg.h:36-38). */
+int hpc_pcg_d(hpc_ctx* ctx, int level, double lc, int nb_relax, int t, double* fd_norm);
+/* cycle_u (mechanical_multigrid.cpp:18-54). */
+int hpc_cycle_u(hpc_ctx* ctx, int level, const hpc_mg* mg, double small_k, double Ut, int t, double* f_norm);
+/* cycle_d (phase_field_multigrid.cpp:18-44). */
+int hpc_cycle_d(hpc_ctx* ctx, int level, const hpc_mg* mg, double lc, int t, double* fd_norm);
+/* u_entire (mechanical_displacement.cpp:25-115): cycles and finest smoother iterations returned. */
+int hpc_u_entire(hpc_ctx* ctx, const hpc_mg* mg, double small_k, double Ut, int t, double* f_norm,
+                 double mech_tol, int* cycles, int* iters);
+/* phase_field (phase_field.cpp:15-57). */
+int hpc_phase_field(hpc_ctx* ctx, const hpc_mg* mg, double lc, int t, double* fd_norm, double pf_tol,
+                    int* cycles, int* iters);
+/* One staggered increment (crack_propagation.cpp:65-121).  out[8] = {Ut, F (u_proportion*FeW),
+ * delta_d_max, d_max, mech cycles, pf cycles, mech finest iters, pf finest iters}. */
+int hpc_step(hpc_ctx* ctx, const hpc_step_params* p, double* out);
+
+/* ---------------- material, history, reductions ---------------- */
+/* MP_choice (material_selection.cpp:47-65). */
+int hpc_mp_choice(hpc_ctx* ctx);
+/* MP_all_element (material_selection.cpp:100-116). */
+int hpc_mp_all_element(hpc_ctx* ctx, double small_k);
+/* VR_all_level (material_coarse_element.cpp:86-102). */
+int hpc_vr_all_level(hpc_ctx* ctx, int field);
+/* Voigt_all_level (material_coarse_element.cpp:106-118). */
+int hpc_voigt_all_level(hpc_ctx* ctx, int field);
+/* coarse_VR (image_input.cpp:244-260). */
+int hpc_coarse_vr(hpc_ctx* ctx, int field);
+/* strain_history (strain_history.cpp:162-210). */
+int hpc_strain_history(hpc_ctx* ctx, double lc, double u_proportion);
+/* fd_h (phase_field_right_hand_side.cpp:14-47). */
+int hpc_fd_h(hpc_ctx* ctx, int level);
+/* delta_d_max / d_max (phase_field_max_search.cpp:17-53). */
+int hpc_delta_d_max(hpc_ctx* ctx, double* out);
+int hpc_d_max(hpc_ctx* ctx, double* out);
+/* U_e (strain_history.cpp:86-131). */
+int hpc_U_e(hpc_ctx* ctx, double lc, double* out);
+/* externe_force_nodal / externe_force_sum (mechanical_right_hnd.cpp:18-59). */
+int hpc_externe_force_nodal(hpc_ctx* ctx, double Ut, double small_k);
+int hpc_externe_force_sum(hpc_ctx* ctx, double* out);
+/* initial_crack (strain_history.cpp:30-70). */
+int hpc_initial_crack(hpc_ctx* ctx, double H_crack, int level);
+
+/* ---------------- boundary conditions (boundary_conditions.cpp:20-154) ---------------- */
+int hpc_dirichlet_bd(hpc_ctx* ctx, int level, int field, double Ut);
+int hpc_dirichlet_force(hpc_ctx* ctx, int level, int f_field, int fi_field);
+int hpc_dirichlet_residual(hpc_ctx* ctx, int level, int field);
+
+/* ---------------- inter-grid transfers (multigrid_intergrid.cpp) ---------------- */
+/* solution_injection (:25-90): level lf-1 of `field` from level lf. */
+int hpc_solution_injection(hpc_ctx* ctx, int field, int comp, int lf);
+/* coarsen_f_standard_routine (:124-342): fc(lf-1) = Fic(lf-1) + full weighting of rf(lf). */
+int hpc_coarsen_f_standard(hpc_ctx* ctx, int fc_field, int rf_field, int fic_field, int comp, int lf);
+/* refine_standard_routine (:416-520): uf(lf) += P (uc(lf-1) - ucold(lf-1)). */
+int hpc_refine_standard(hpc_ctx* ctx, int uf_field, int uc_field, int ucold_field, int comp, int lf);
+
+/* ---------------- input path (image_input.cpp:120-282, csv_reader.cpp) ---------------- */
+/* Raw uint8 image (x fastest, voxel_n[3] voxels) + gray-level table -> finest bulK, G, gc, then the
+ * nodal Voigt-Reuss-Hill hierarchy (coarse_VR). */
+int hpc_image_material(hpc_ctx* ctx, const uint8_t* image, const int* voxel_n, int ngray, const int* gray,
+                       const double* E, const double* nu, const double* gc, double voxel_size);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

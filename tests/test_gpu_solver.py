@@ -1,0 +1,103 @@
+"""Parity of the CUDA smoothers, V-cycles and full staggered increments with the C oracle (GPU).
+
+Plain FP64 form: u and d must match the oracle (itself pinned to the reference) within 1e-10
+relative L2, with the same number of V-cycles.  The cases use a 9^3 coarsest grid (element_nb 8,
+as the reference's configurations do): on smaller coarsest grids the reference's fixed 50-iteration
+coarsest PCG runs past convergence and amplifies rounding differences of any two implementations.
+"""
+import numpy as np
+import pytest
+
+from oracle.bindings import COracle
+from hpcrack_b200 import microstructure as ms
+from hpcrack_b200.solver import Hierarchy
+from cases import BULK, G, GC, D, H, FD, KE, GE, R, U, FU, RU, load_random, load_workload, rel
+
+pytestmark = pytest.mark.gpu
+MG_U = (50, 4, 2, 1, 12)
+MG_D = (10, 2, 1, 1, 12)
+
+
+def _pair(ml, enb, seed=7):
+    gpu = Hierarchy(ml, enb)
+    orc = COracle(ml, enb)
+    load_random([gpu, orc], ml, enb, seed)
+    return gpu, orc
+
+
+@pytest.mark.parametrize("level,t", [(1, 0), (1, 3), (0, 2)])
+def test_pcg_u_single(level, t):
+    gpu, orc = _pair(1, (8, 8, 8))
+    fn_g = fn_o = 0.0
+    for nb in (1, 4):
+        _, fn_g = gpu.pcg_u(level, 1e-5, 1.0, nb, t, fn_g)
+        _, fn_o = orc.pcg_u(level, 1e-5, 1.0, nb, t, fn_o)
+        assert rel(gpu.get(U, level), orc.get(U, level)) < 1e-12
+        assert rel(gpu.get(RU, level), orc.get(RU, level)) < 1e-10
+        assert abs(fn_g - fn_o) <= 1e-12 * max(abs(fn_o), 1.0)
+
+
+def test_pcg_d_single():
+    gpu, orc = _pair(1, (8, 8, 8))
+    for impl in (gpu, orc):
+        impl.fd_h(1)
+    fg = fo = 0.0
+    for nb in (1, 3):
+        _, fg = gpu.pcg_d(1, 2.0, nb, 0, fg)
+        _, fo = orc.pcg_d(1, 2.0, nb, 0, fo)
+        assert rel(gpu.get(D, 1), orc.get(D, 1)) < 1e-12
+        assert abs(fg - fo) <= 1e-12 * abs(fo)
+
+
+def test_cycles():
+    gpu, orc = _pair(2, (8, 8, 8))
+    for impl in (gpu, orc):
+        impl.mp_all_element(1e-5)
+        impl.vr_all_level(KE)
+        impl.vr_all_level(GE)
+        for l in range(3):
+            impl.fd_h(l)
+    fg = fo = 0.0
+    _, fg = gpu.cycle_u(2, MG_U, 1e-5, 1.0, 0, fg)
+    _, fo = orc.cycle_u(2, MG_U, 1e-5, 1.0, 0, fo)
+    assert rel(gpu.get(U, 2), orc.get(U, 2)) < 1e-10
+    assert abs(fg - fo) <= 1e-10 * abs(fo)
+    dg = do = 0.0
+    _, dg = gpu.cycle_d(2, MG_D, 2.0, 0, dg)
+    _, do = orc.cycle_d(2, MG_D, 2.0, 0, do)
+    assert rel(gpu.get(D, 2), orc.get(D, 2)) < 1e-10
+
+
+@pytest.mark.parametrize("name,steps", [("small17", 4), ("small33", 3)])
+def test_staggered_steps(name, steps):
+    w = ms.make_workload(name)
+    gpu = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start)
+    orc = COracle(w.maxlevel, w.element_nb, x0=w.x_start)
+    load_workload([gpu, orc], w)
+    for l in range(w.maxlevel + 1):
+        for f in (BULK, G, GC):
+            assert rel(gpu.get(f, l), orc.get(f, l)) == 0.0, (l, f)
+    L = w.maxlevel
+    for t in range(steps):
+        og = gpu.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
+                      mech_tol=1e-6, pf_tol=1e-12)
+        oo = orc.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
+                      mech_tol=1e-6, pf_tol=1e-12)
+        assert og[4] == oo[4] and og[5] == oo[5], (t, og, oo)  # V-cycle counts
+        assert rel(gpu.get(U, L), orc.get(U, L)) < 1e-10, t
+        assert rel(gpu.get(D, L), orc.get(D, L)) < 1e-10, t
+        assert rel(gpu.get(H, L), orc.get(H, L)) < 1e-10, t
+        assert abs(og[1] - oo[1]) <= 1e-10 * max(abs(oo[1]), 1e-300), t
+        assert abs(og[3] - oo[3]) <= 1e-10 * max(abs(oo[3]), 1e-300), t
+
+
+def test_reference_schedule_Ue():
+    """t == 0 with the reference's Ue-based schedule (crack_propagation.cpp:71-80)."""
+    w = ms.make_workload("small17")
+    gpu = Hierarchy(w.maxlevel, w.element_nb)
+    orc = COracle(w.maxlevel, w.element_nb)
+    load_workload([gpu, orc], w)
+    og = gpu.step(0, w.mg_u, w.mg_d, 1e-5, w.lc, w.voxel_size)
+    oo = orc.step(0, w.mg_u, w.mg_d, 1e-5, w.lc, w.voxel_size)
+    assert abs(og[0] - oo[0]) <= 1e-10 * oo[0]
+    assert og[4] == oo[4]

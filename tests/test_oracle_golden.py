@@ -1,0 +1,143 @@
+"""Pins the C oracle (oracle/hpc_oracle.c) to the reference's golden vectors (CPU).
+
+tests/golden/*.npz were produced by the reference HPCrack sources themselves (compiled by
+oracle/Makefile, driven by tests/golden/make_golden.py).  The oracle replays the same inputs;
+it differs from the reference only in the order of the element scatter and of global sums, so
+the bar is 1e-13 relative L2 on single operators, bit equality on integer/flag outputs, and
+1e-10 on multi-step solves (the plain-form parity bar).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle.bindings import COracle
+from oracle import bindings as B
+from hpcrack_b200 import microstructure as ms
+from cases import rel
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+SMALL_K = 1e-5
+LC = 2.0
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLD, f"{name}.npz"), allow_pickle=False))
+
+
+def replay_inputs(g):
+    ml = int(g["ml"])
+    enb = tuple(int(v) for v in g["enb"])
+    x0 = tuple(float(v) for v in g["x0"]) if "x0" in g else (0.0, 0.0, 0.0)
+    orc = COracle(ml, enb, x0=x0)
+    for l in range(ml + 1):
+        for k in (B.BULK, B.G, B.GC, B.D, B.H, B.KE, B.GE):
+            orc.set(k, l, g[f"in_{k}_{l}"])
+        orc.set_choice(l, g[f"in_choice_{l}"])
+        orc.set(B.U, l, g[f"in_u_{l}"])
+        orc.set(B.FU, l, g[f"in_fu_{l}"])
+    return orc, ml
+
+
+@pytest.mark.parametrize("case", ["ops_iso", "ops_xwide", "ops_ywide"])
+def test_operators_match_reference(case):
+    g = load(case)
+    orc, ml = replay_inputs(g)
+    for l in range(ml + 1):
+        orc.internal_force(l, B.U, B.RU, SMALL_K)
+        assert rel(orc.get(B.RU, l), g[f"if_{l}"]) < 1e-13
+        orc.prem_u(l, B.RU, SMALL_K)
+        assert rel(orc.get(B.RU, l), g[f"prem_{l}"]) < 1e-13
+        orc.fld(l, B.D, B.FD, LC)
+        assert rel(orc.get(B.FD, l), g[f"fld_{l}"]) < 1e-13
+        orc.precondition_m(l, B.R, LC)
+        assert rel(orc.get(B.R, l), g[f"pm_{l}"]) < 1e-13
+        orc.fd_h(l)
+        assert np.array_equal(orc.get(B.FD, l), g[f"fdh_{l}"])  # same sequential order: bit-identical
+    lf = ml
+    if lf >= 1:
+        orc.solution_injection(B.U, 1, lf)
+        assert np.array_equal(orc.get(B.U, lf - 1)[1], g["inject"])
+        orc.coarsen_f_standard(B.RU, B.FU, B.UOLD, 1, lf)
+        assert np.array_equal(orc.get(B.RU, lf - 1)[1], g["restrict"])
+        orc.set(B.UOLD, lf - 1, g["in_uold"])
+        orc.refine_standard(B.FU, B.U, B.UOLD, 1, lf)
+        assert np.array_equal(orc.get(B.FU, lf)[1], g["prolong"])
+    orc.dirichlet_bd(ml, B.U, 0.37)
+    assert np.array_equal(orc.get(B.U, ml), g["bc_u"])
+    orc.dirichlet_force(ml, B.FU, B.U)
+    assert np.array_equal(orc.get(B.FU, ml), g["bc_force"])
+    orc.dirichlet_residual(ml, B.FU)
+    assert np.array_equal(orc.get(B.FU, ml), g["bc_res"])
+    orc.mp_choice()
+    nx, ny, nz = orc.dims[ml]
+    elem = np.zeros((nz, ny, nx), bool)
+    elem[:-1, :-1, :-1] = True
+    elem = elem.ravel()
+    assert np.array_equal(orc.get_choice(ml)[elem], g["choice"][elem])
+    orc.mp_all_element(SMALL_K)
+    assert rel(orc.get(B.KE, ml)[elem], g["ke"][elem]) < 1e-13
+    assert rel(orc.get(B.GE, ml)[elem], g["ge"][elem]) < 1e-13
+    orc.vr_all_level(B.KE)
+    ke = np.concatenate([orc.get(B.KE, l) for l in range(ml + 1)])
+    assert rel(ke, g["ke_vr"]) < 1e-13
+    orc.coarse_vr(B.GC)
+    gc = np.concatenate([orc.get(B.GC, l) for l in range(ml + 1)])
+    assert np.array_equal(gc, g["gc_vr"])
+    orc.strain_history(LC, 3.5)
+    assert rel(orc.get(B.H, ml), g["H_hist"]) < 1e-13
+    orc.voigt_all_level(B.H)
+    Hv = np.concatenate([orc.get(B.H, l) for l in range(ml + 1)])
+    assert rel(Hv, g["H_voigt"]) < 1e-13
+    assert abs(orc.U_e(LC) - float(g["ue"])) <= 1e-13 * abs(float(g["ue"]))
+    assert orc.d_max() == float(g["dmax"])
+    assert orc.delta_d_max() == float(g["ddmax"])
+    orc.externe_force_nodal(0.37, SMALL_K)
+    assert rel(orc.get(B.FU, ml), g["reaction"]) < 1e-13
+    assert abs(orc.externe_force_sum() - float(g["fsum"])) <= 1e-12 * max(1.0, abs(float(g["fsum"])))
+    orc.close()
+
+
+def test_smoothers_and_cycles_match_reference():
+    g = load("solver")
+    ml, enb = int(g["ml"]), tuple(int(v) for v in g["enb"])
+    orc = COracle(ml, enb)
+    from cases import load_random
+    load_random([orc], ml, enb, int(g["seed"]))
+    _, fn = orc.pcg_u(1, SMALL_K, 1.0, 4, 0, 0.0)
+    assert rel(orc.get(B.U, 1), g["pcg_u_u"]) < 1e-12
+    assert abs(fn - float(g["pcg_u_fnorm"])) <= 1e-12 * abs(float(g["pcg_u_fnorm"]))
+    _, fdn = orc.pcg_d(1, LC, 3, 0, 0.0)
+    assert rel(orc.get(B.D, 1), g["pcg_d_d"]) < 1e-12
+    orc.mp_all_element(SMALL_K)
+    orc.vr_all_level(B.KE)
+    orc.vr_all_level(B.GE)
+    _, fn = orc.cycle_u(1, (50, 4, 2, 1, 12), SMALL_K, 1.0, 0, fn)
+    assert rel(orc.get(B.U, 1), g["cycle_u_u"]) < 1e-10
+    _, fdn = orc.cycle_d(1, (10, 2, 1, 1, 12), LC, 0, fdn)
+    assert rel(orc.get(B.D, 1), g["cycle_d_d"]) < 1e-10
+    orc.close()
+
+
+@pytest.mark.parametrize("case,reference_schedule", [("steps17", False), ("steps17_ue", True)])
+def test_staggered_increments_match_reference(case, reference_schedule):
+    g = load(case)
+    w = ms.make_workload(str(g["name"]))
+    orc = COracle(w.maxlevel, w.element_nb, x0=w.x_start)
+    orc.image_material(w.image, w.nodes, w.table(), w.voxel_size)
+    L = w.maxlevel
+    for f, key in ((B.BULK, "bulk"), (B.G, "g"), (B.GC, "gc")):
+        # the reference's input path (raw file + CSV) against the oracle's restatement: bit-identical
+        assert np.array_equal(np.concatenate([orc.get(f, l) for l in range(L + 1)]), g[key])
+    kw = {} if reference_schedule else {"ut0": w.ut0, "dU": w.du}
+    for t in range(int(g["steps"])):
+        o = orc.step(t, w.mg_u, w.mg_d, SMALL_K, w.lc, w.voxel_size, **kw)
+        go = g[f"out_{t}"]
+        assert o[4] == go[4] and o[5] == go[5], (t, o, go)       # V-cycle counts
+        assert o[6] == go[6] and o[7] == go[7], (t, o, go)       # finest smoother iterations
+        assert rel(orc.get(B.U, L), g[f"u_{t}"]) < 1e-10, t
+        assert rel(orc.get(B.D, L), g[f"d_{t}"]) < 1e-10, t
+        assert rel(orc.get(B.H, L), g[f"H_{t}"]) < 1e-10, t
+        assert abs(o[1] - go[1]) <= 1e-10 * max(abs(go[1]), 1e-300), t
+    assert np.allclose(orc.state(), g["state"], rtol=1e-10, atol=0)
+    orc.close()
