@@ -65,30 +65,9 @@ def dist_setup():
     return rank, world, local
 
 
-def reduce_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def reduce_sum(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
-
-
 def barrier(world: int):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from hpcrack_b200 import replicas
+    replicas.barrier(world)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -251,6 +230,7 @@ def peaks():
 def run_b200(args, rank, world, local):
     import torch
     from hpcrack_b200 import microstructure as ms
+    from hpcrack_b200 import replicas
     from hpcrack_b200.solver import KC_MECH_PCG_FINEST, U, D, H, FU, DOLDF
 
     torch.cuda.set_device(local)
@@ -296,8 +276,7 @@ def run_b200(args, rank, world, local):
 
     dof_iters = sum(3.0 * N * o[6] + 1.0 * N * o[7] for o in outs)
     mech_cycles = sum(o[4] for o in outs)
-    max_ms = reduce_max(ms_total, world)
-    tot_dof_iters = reduce_sum(dof_iters, world)
+    max_ms, tot_dof_iters = replicas.aggregate(ms_total, dof_iters, world)
     value = tot_dof_iters / (max_ms / 1e3) / 1e6
 
     # roofline of the dominant kernel: fused direction update + K(d) p + (p, w) on the finest level.
@@ -350,8 +329,8 @@ def run_b200(args, rank, world, local):
         f1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
-        e2e_ms = reduce_max(f0.elapsed_time(f1), world)
-        e2e_val = reduce_sum(e2e_iters, world) / (e2e_ms / 1e3) / 1e6
+        e2e_ms, e2e_work = replicas.aggregate(f0.elapsed_time(f1), e2e_iters, world)
+        e2e_val = e2e_work / (e2e_ms / 1e3) / 1e6
         e2e = {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": 8 * N * 9, "d2h_bytes_per_step": 8 * N * 8,
                "ms_per_step": e2e_ms / args.steps}
         del hu, hfu, hd, hH, hdo

@@ -1,7 +1,7 @@
 // Element-operator kernels: mechanical K(d) u and diag K(d), phase-field A_d x and diag A_d, with
 // fused epilogues (residual, PCG direction update, FAS right-hand side, reactions).
 //
-// Tiling ("warp strip"): each warp owns a strip of 32 element columns in x (31 output nodes),
+// Tiling ("warp strip"): each warp owns a strip of 32 node columns in x (31 elements, 30 output nodes),
 // WY element rows in y (WY-1 output node rows) and CZ output node planes in z, and marches in z.
 // Per element row a lane computes one element; the x-neighbour contributions are combined with
 // one shuffle, y-neighbours through registers (the previous row's upper-face sums) and
@@ -19,7 +19,7 @@ namespace hpc {
 constexpr int kWarps = 4;    // warps per block
 constexpr int kWY = 8;       // element rows per strip (kWY - 1 output node rows)
 constexpr int kCZ = 16;      // output planes per strip
-constexpr int kOX = 31;      // output nodes per strip in x
+constexpr int kOX = 30;      // output nodes per strip in x (lanes 1..30)
 
 struct StripGeo {
   int tx, ty, tz;            // strips per axis
@@ -49,7 +49,7 @@ struct MechK {
   const int8_t* choice;
   double small_k;
   double* fu;
-  const double* preM;
+  const double* invM;
   const double* r;
   double* p_new;
   const double* rf;
@@ -75,7 +75,7 @@ __device__ __forceinline__ MechNode mech_load(const MechK& k, int x, int y, int 
       double pv = 0.0;
       if (ok) {
         const long long o = n + (long long)m * k.g.n;
-        const double zv = k.r[o] / k.preM[o];
+        const double zv = k.r[o] * k.invM[o];
         pv = k.first ? zv : fma(beta, k.src[o], zv);
       }
       v.u[m] = pv;
@@ -178,15 +178,10 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
             for (int m = 0; m < 3; ++m) t.u[m] = shfl_down1(o.u[m]);
             if (FINEST) { t.K = shfl_down1(o.K); t.G = shfl_down1(o.G); t.d = shfl_down1(o.d); }
           }
-        if (lane == 31) {
-#pragma unroll
-          for (int c = 0; c < 2; ++c)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) nd[1 + 2 * b + 4 * c] = mech_load<FINEST, EPI>(k, x + 1, ey + b, kk + c, beta);
-        }
-        // ---- element contribution
+        // ---- element contribution (lane 31 has no right neighbour: its element belongs to the next strip)
         double f[3][8];
-        const bool valid = x >= 0 && x <= k.g.nx - 2 && ey >= 0 && ey <= k.g.ny - 2 && kk >= 0 && kk <= k.g.nz - 2;
+        const bool valid = lane < 31 && x >= 0 && x <= k.g.nx - 2 && ey >= 0 && ey <= k.g.ny - 2 && kk >= 0 &&
+                           kk <= k.g.nz - 2;
         if (valid) {
           const long long e = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
           double Kw[8], Gw[8];
@@ -227,7 +222,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
             tot[m] = *zp + yp[0][m] + X[0][0][m];
             *zp = yp[1][m] + X[0][1][m];
           }
-          if (kk >= z0 && lane >= 1 && x < k.g.nx && ey < k.g.ny) {
+          if (kk >= z0 && lane >= 1 && lane <= 30 && x < k.g.nx && ey < k.g.ny) {
             const long long n = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
             const long long N = k.g.n;
             if (EPI == EPI_PLAIN) {
@@ -246,7 +241,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
                 red0 = fma(fv, fv, red0);
                 double rv = fix[m] ? 0.0 : fv - tot[m];
                 k.out[n + m * N] = rv;
-                if (k.preM) red1 = fma(rv, rv / k.preM[n + m * N], red1);
+                if (k.invM) red1 = fma(rv, rv * k.invM[n + m * N], red1);
                 red2 = fma(rv, rv, red2);
               }
             } else if (EPI == EPI_PCG) {
@@ -384,7 +379,7 @@ int launch_mech(hpc_ctx* c, const MechCall& m) {
   k.small_k = m.small_k;
   k.fu = m.fu;
   k.set_fnorm = m.set_fnorm;
-  k.preM = m.preM;
+  k.invM = m.invM;
   k.r = m.r;
   k.p_new = m.p_new;
   k.first = m.first;
@@ -437,7 +432,7 @@ struct PfK {
   const double *gc, *H;
   double lc;
   const double* fd;
-  const double* preM;
+  const double* invM;
   const double* r;
   double* p_new;
   const double* rf;
@@ -457,7 +452,7 @@ __device__ __forceinline__ PfNode pf_load(const PfK& k, int x, int y, int z, dou
   if (EPI == EPI_PCG) {
     double pv = 0.0;
     if (ok) {
-      const double zv = k.r[n] / k.preM[n];
+      const double zv = k.r[n] * k.invM[n];
       pv = k.first ? zv : fma(beta, k.src[n], zv);
     }
     v.x = pv;
@@ -504,14 +499,9 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
             nd[1 + 2 * b + 4 * c].x = shfl_down1(nd[2 * b + 4 * c].x);
             nd[1 + 2 * b + 4 * c].gc = shfl_down1(nd[2 * b + 4 * c].gc);
           }
-        if (lane == 31) {
-#pragma unroll
-          for (int c = 0; c < 2; ++c)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) nd[1 + 2 * b + 4 * c] = pf_load<EPI>(k, x + 1, ey + b, kk + c, beta);
-        }
         double f[8];
-        const bool valid = x >= 0 && x <= k.g.nx - 2 && ey >= 0 && ey <= k.g.ny - 2 && kk >= 0 && kk <= k.g.nz - 2;
+        const bool valid = lane < 31 && x >= 0 && x <= k.g.nx - 2 && ey >= 0 && ey <= k.g.ny - 2 && kk >= 0 &&
+                           kk <= k.g.nz - 2;
         if (valid) {
           const long long e = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
           double gcn[8], gcg[8], aw[8], bw[8];
@@ -548,7 +538,7 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
           double* zp = zc + (rr - 1) * 32 + lane;
           const double tot = *zp + yp[0] + X[0][0];
           *zp = yp[1] + X[0][1];
-          if (kk >= z0 && lane >= 1 && x < k.g.nx && ey < k.g.ny) {
+          if (kk >= z0 && lane >= 1 && lane <= 30 && x < k.g.nx && ey < k.g.ny) {
             const long long n = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
             if (EPI == EPI_PLAIN) {
               k.out[n] = tot;
@@ -558,7 +548,7 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
               k.out[n] = rv;
               red0 = fma(fv, fv, red0);
               red1 = fma(rv, rv, red1);
-              if (k.preM) red2 = fma(rv, rv / k.preM[n], red2);
+              if (k.invM) red2 = fma(rv, rv * k.invM[n], red2);
             } else if (EPI == EPI_PCG) {
               k.out[n] = tot;
               k.p_new[n] = own00;
@@ -645,7 +635,7 @@ int launch_pf(hpc_ctx* c, const PfCall& p) {
   k.H = c->F[p.level].H;
   k.lc = p.lc;
   k.fd = p.fd;
-  k.preM = p.preM;
+  k.invM = p.invM;
   k.r = p.r;
   k.p_new = p.p_new;
   k.rf = p.rf;

@@ -197,6 +197,7 @@ static int mech_diags(hpc_ctx* c, int top, double small_k) {
     int rc = launch_mech_diag(c, l, is_finest(c, l), small_k, c->F[l].preMu);
     if (rc) return rc;
     if ((rc = launch_zero_count(c, l, 3, c->F[l].preMu, S_ZEROS + l))) return rc;
+    if ((rc = launch_invert(c, l, 3, c->F[l].preMu))) return rc;
   }
   return check_zero_diags(c, top, "PreM_u");
 }
@@ -205,6 +206,7 @@ static int pf_diags(hpc_ctx* c, int top, double lc) {
     int rc = launch_pf_diag(c, l, lc, c->F[l].preMd);
     if (rc) return rc;
     if ((rc = launch_zero_count(c, l, 1, c->F[l].preMd, S_ZEROS + l))) return rc;
+    if ((rc = launch_invert(c, l, 1, c->F[l].preMd))) return rc;
   }
   return check_zero_diags(c, top, "Precondition_M");
 }
@@ -224,7 +226,7 @@ static int pcg_u_dev(hpc_ctx* c, int l, double small_k, double Ut, int nb, int t
   m.small_k = small_k;
   m.fu = F.fu;
   m.set_fnorm = (t == 0 && m.finest);
-  m.preM = F.preMu;
+  m.invM = F.preMu;
   m.s_out0 = m.set_fnorm ? S_FNORM : -1;
   m.s_out1 = slot_rz(0);
   m.s_out2 = S_RNORM;
@@ -239,7 +241,7 @@ static int pcg_u_dev(hpc_ctx* c, int l, double small_k, double Ut, int nb, int t
     q.src = p_old;
     q.out = F.w;
     q.small_k = small_k;
-    q.preM = F.preMu;
+    q.invM = F.preMu;
     q.r = F.ru;
     q.p_new = p_new;
     q.first = it == 0;
@@ -265,7 +267,7 @@ static int pcg_d_dev(hpc_ctx* c, int l, double lc, int nb) {
   m.out = F.R;
   m.lc = lc;
   m.fd = F.fd;
-  m.preM = F.preMd;
+  m.invM = F.preMd;
   m.s_out0 = S_FDNORM;
   m.s_out1 = S_RNORM;
   m.s_out2 = slot_rz(0);
@@ -279,7 +281,7 @@ static int pcg_d_dev(hpc_ctx* c, int l, double lc, int nb) {
     q.src = p_old;
     q.out = F.wd;
     q.lc = lc;
-    q.preM = F.preMd;
+    q.invM = F.preMd;
     q.r = F.R;
     q.p_new = p_new;
     q.first = it == 0;
@@ -382,7 +384,7 @@ static int u_entire_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut,
   m.small_k = small_k;
   m.fu = c->F[L].fu;
   m.set_fnorm = false;
-  m.preM = nullptr;
+  m.invM = nullptr;
   m.s_out0 = m.s_out1 = -1;
   m.s_out2 = S_RNORM;
   if ((rc = launch_mech(c, m))) return rc;
@@ -833,6 +835,7 @@ int hpc_pcg_u(hpc_ctx* c, int level, double small_k, double Ut, int nb_relax, in
   if ((rc = launch_mech_diag(c, level, is_finest(c, level), small_k, c->F[level].preMu))) return rc;
   if ((rc = launch_zero_count(c, level, 3, c->F[level].preMu, S_ZEROS))) return rc;
   if (nb_relax > 0 && (rc = check_zero_diags(c, 0, "PreM_u"))) return rc;
+  if ((rc = launch_invert(c, level, 3, c->F[level].preMu))) return rc;
   if ((rc = pcg_u_dev(c, level, small_k, Ut, nb_relax, t))) return rc;
   if ((rc = read_scalars(c, S_FNORM, 1, f_norm))) return rc;
   return HPC_OK;
@@ -865,6 +868,7 @@ int hpc_pcg_d(hpc_ctx* c, int level, double lc, int nb_relax, int t, double* fd_
   if ((rc = launch_pf_diag(c, level, lc, c->F[level].preMd))) return rc;
   if ((rc = launch_zero_count(c, level, 1, c->F[level].preMd, S_ZEROS))) return rc;
   if (nb_relax > 0 && (rc = check_zero_diags(c, 0, "Precondition_M"))) return rc;
+  if ((rc = launch_invert(c, level, 1, c->F[level].preMd))) return rc;
   if ((rc = pcg_d_dev(c, level, lc, nb_relax))) return rc;
   return read_scalars(c, S_FDNORM, 1, fd_norm);
 }

@@ -37,8 +37,8 @@ struct LevelFields {
   double *u, *fu, *ru, *uold;  // 3n each; component c at +c*n
   int8_t* choice;
   // work arrays
-  double *preMu, *p, *w, *tmp3;  // 3n
-  double *preMd, *pd, *wd, *tmp1;  // n
+  double *preMu, *p, *w, *tmp3;  // 3n; preMu holds the inverse diagonal while a solve runs
+  double *preMd, *pd, *wd, *tmp1;  // n;  preMd likewise
   uint8_t* bc_host_copy;           // host copies of the axis flags (nx+ny+nz bytes)
 };
 
@@ -126,8 +126,8 @@ struct MechCall {
   // RESIDUAL: r = fu - K u, zero at Dirichlet nodes; optionally fu[bc] = (K u)[bc] and f_norm.
   double* fu;
   bool set_fnorm;     // t == 0 on the finest level (mechanical_pcg.cpp:252-258)
-  const double* preM; // RESIDUAL: rz = sum r^2/preM ; PCG: z = r/preM
-  // PCG: p_new = r/preM + beta p_old with beta = scal[s_rz]/scal[s_rz_prev] (0 if first)
+  const double* invM; // inverse diagonal; RESIDUAL: rz = sum r^2 invM ; PCG: z = r invM
+  // PCG: p_new = r invM + beta p_old with beta = scal[s_rz]/scal[s_rz_prev] (0 if first)
   const double* r;
   double* p_new;
   int s_rz, s_rz_prev, first;
@@ -147,7 +147,7 @@ struct PfCall {
   double* out;
   double lc;
   const double* fd;     // RESIDUAL: R = fd - A d
-  const double* preM;   // PCG
+  const double* invM;   // inverse diagonal (PCG, and rz in RESIDUAL)
   const double* r;
   double* p_new;
   int s_rz, s_rz_prev, first;
@@ -170,6 +170,8 @@ int launch_bc(hpc_ctx* c, int level, double* v, const double* src, int kind, dou
 int launch_dot(hpc_ctx* c, int level, int ncomp, const double* a, const double* b, int slot);
 // fill / copy helpers over padded levels
 int launch_fill(hpc_ctx* c, double* v, long long n, double value);
+// v = 1/v on the valid nodes of a level (ncomp components)
+int launch_invert(hpc_ctx* c, int level, int ncomp, double* v);
 int launch_axpby(hpc_ctx* c, double* y, const double* a, const double* b, double sa, double sb, long long n);
 // Transfers
 int launch_inject(hpc_ctx* c, int lf, const double* f, double* co, int ncomp);

@@ -45,7 +45,7 @@ __device__ __forceinline__ long long nidx(const LevelGeo& g, int i, int j, int k
 // PCG updates (mechanical_pcg.cpp:301-321, phase_field_pcg.cpp:192-200)
 // ---------------------------------------------------------------------------------------------
 __global__ void mech_update_kernel(LevelGeo g, double* u, double* r, const double* p, const double* w,
-                                   const double* preM, int s_rz, int s_pw, RedTarget red) {
+                                   const double* invM, int s_rz, int s_pw, RedTarget red) {
   const double alpha = red.scal[s_rz] / red.scal[s_pw];
   double rz = 0.0, rn = 0.0;
   FOR_NODES(g) {
@@ -58,7 +58,7 @@ __global__ void mech_update_kernel(LevelGeo g, double* u, double* r, const doubl
       u[o] = fma(p[o], alpha, u[o]);
       double rv = fix[m] ? 0.0 : fma(-w[o], alpha, r[o]);
       r[o] = rv;
-      rz = fma(rv, rv / preM[o], rz);
+      rz = fma(rv, rv * invM[o], rz);
       rn = fma(rv, rv, rn);
     }
   }
@@ -80,7 +80,7 @@ int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_p
 }
 
 __global__ void pf_update_kernel(LevelGeo g, double* d, double* r, const double* p, const double* w,
-                                 const double* preM, int s_rz, int s_pw, RedTarget red) {
+                                 const double* invM, int s_rz, int s_pw, RedTarget red) {
   const double alpha = red.scal[s_rz] / red.scal[s_pw];
   double rz = 0.0, rn = 0.0;
   FOR_NODES(g) {
@@ -88,7 +88,7 @@ __global__ void pf_update_kernel(LevelGeo g, double* d, double* r, const double*
     d[n] = fma(p[n], alpha, d[n]);
     const double rv = fma(-w[n], alpha, r[n]);
     r[n] = rv;
-    rz = fma(rv, rv / preM[n], rz);
+    rz = fma(rv, rv * invM[n], rz);
     rn = fma(rv, rv, rn);
   }
   double v[3] = {rz, rn, 0.0};
@@ -167,6 +167,19 @@ int launch_fill(hpc_ctx* c, double* v, long long n, double value) {
   int grid = (int)(blocks < num_sms_v() * 16LL ? blocks : num_sms_v() * 16LL);
   if (grid <= 0) return HPC_OK;
   fill_kernel<<<grid, 256, 0, c->stream>>>(v, n, value);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+
+__global__ void invert_kernel(LevelGeo g, int ncomp, double* v) {
+  FOR_NODES(g) {
+    const long long n = nidx(g, i, j, kz);
+    for (int m = 0; m < ncomp; ++m) v[n + m * g.n] = 1.0 / v[n + m * g.n];
+  }
+}
+int launch_invert(hpc_ctx* c, int level, int ncomp, double* v) {
+  const LevelGeo& g = c->L[level];
+  invert_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, ncomp, v);
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
 }

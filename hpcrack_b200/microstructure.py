@@ -172,10 +172,11 @@ def make_workload(name: str) -> Workload:
         return Workload(name, img, (8, 8, 8), maxlevel_for(n, 0, 8), (0.0, 0.0, 0.0), 1e-6, 2.0, 1e-6,
                         (50, 4, 2, 1, 200), (10, 2, 1, 1, 200), 3, ut0=1e-4 * (n - 1), du=1e-4 * (n - 1),
                         mech_tol=1e-16, pf_tol=1e-16)
-    if name == "plain257":
-        n = 257
-        img = sphere_image((n, n, n), 1, [Phase(INCLUSION_GRAY, 6, 20, volume_fraction=0.25),
-                                          Phase(PORE_GRAY, 3, 8, volume_fraction=0.05)])
+    if name in ("plain257", "mid129"):
+        n = 257 if name == "plain257" else 129
+        s = (n - 1) / 256.0
+        img = sphere_image((n, n, n), 1, [Phase(INCLUSION_GRAY, 6 * s, 20 * s, volume_fraction=0.25),
+                                          Phase(PORE_GRAY, max(3 * s, 1.5), 8 * s, volume_fraction=0.05)])
         return Workload(name, img, (8, 8, 8), maxlevel_for(n, 0, 8), (0.0, 0.0, 0.0), 1e-6, 2.0, 1e-6,
                         (50, 4, 2, 1, 200), (10, 2, 1, 1, 200), 20, ut0=1e-4 * (n - 1), du=1e-4 * (n - 1),
                         mech_tol=1e-16, pf_tol=1e-16, crack={"H": 1e6, "layer": (n - 1) // 2, "xfrac": 0.5})
@@ -204,9 +205,11 @@ def precrack_fields(w: Workload):
     return H.ravel(), d.ravel()
 
 
-def write_inputs(w: Workload, directory: str) -> dict:
+def write_inputs(w: Workload, directory: str, extra: dict | None = None) -> dict:
     """Writes the reference's inputs for this workload: raw image, data/Material_Property.csv and a
-    config.txt (keys written without spaces around '=', which the reference's parser requires)."""
+    config.txt (keys written without spaces around '=', which the reference's parser requires;
+    configuration.cpp:25 compares the whole text left of '=').  `extra` adds key=value lines
+    (e.g. outTdata, Tdatafrequence, outK)."""
     os.makedirs(os.path.join(directory, "data"), exist_ok=True)
     raw = os.path.join(directory, "data", f"{w.name}.raw")
     w.image.tofile(raw)
@@ -226,4 +229,6 @@ def write_inputs(w: Workload, directory: str) -> dict:
             nu0, nu1, nu2, gamma, ncy = vals
             f.write(f"ncy_{key}={ncy}\nnu0_{key}={nu0}\nnu1_{key}={nu1}\nnu2_{key}={nu2}\ngamma_{key}={gamma}\n")
         f.write(f"lc={int(w.lc)}\n")
+        for k, v in (extra or {}).items():
+            f.write(f"{k}={v}\n")
     return {"raw": raw, "config": cfg}
