@@ -45,7 +45,23 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-timing", action="store_true")
+    ap.add_argument("--kernel-only", type=int, default=0, metavar="NB",
+                    help="profiling driver: set the specimen up, run one finest-level pcg_u with NB iterations "
+                         "(NB launches of the dominant kernel) and exit")
     return ap.parse_args()
+
+
+def run_kernel_only(args, local):
+    """A short, bounded program for profilers: material setup, then pcg_u(NB) on the finest level."""
+    from hpcrack_b200 import microstructure as ms
+    w = ms.make_workload(args.workload)
+    hier = load_specimen(w, local)
+    hier.mp_choice()
+    hier.mp_all_element(w.small_k)
+    _, fn = hier.pcg_u(w.maxlevel, w.small_k, 1.0, args.kernel_only, 0, 0.0)
+    hier.sync()
+    print(json.dumps({"kernel_only": args.kernel_only, "workload": w.name, "f_norm": fn}), flush=True)
+    hier.close()
 
 
 # ---------------------------------------------------------------------------------------------
@@ -361,7 +377,9 @@ def main():
     args = parse_args()
     rank, world, local = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.kernel_only:
+            run_kernel_only(args, local)
+        elif args.impl == "reference":
             run_reference(args, rank, world)
         else:
             run_b200(args, rank, world, local)

@@ -443,4 +443,47 @@ __device__ __host__ __forceinline__ bool choice_in_image(long long b, long long 
   return false;
 }
 
+__device__ __forceinline__ long long nidx(const LevelGeo& g, int i, int j, int k) {
+  return (long long)i + (long long)j * g.px + (long long)k * g.plane;
+}
+
+// Full-weighting restriction of a fine residual at coarse node (fx/2, fy/2, fz/2), neighbours outside
+// the fine grid counted as 0, in the reference's term order (multigrid_intergrid.cpp:124-342).
+__device__ __forceinline__ double full_weight(const LevelGeo& gf, const double* rf, int fx, int fy, int fz) {
+  const int Xl = gf.nx - 2, Yl = gf.ny - 2, Zl = gf.nz - 2;
+  auto R = [&](int a, int b, int c) -> double { return rf[nidx(gf, a, b, c)]; };
+  const bool xm = fx < 1, xp = fx > Xl, ym = fy < 1, yq = fy > Yl, zm = fz < 1, zq = fz > Zl;
+  const double r11 = (xm || ym || zm) ? 0.0 : R(fx - 1, fy - 1, fz - 1);
+  const double r12 = (xm || ym || zq) ? 0.0 : R(fx - 1, fy - 1, fz + 1);
+  const double r13 = (xm || yq || zm) ? 0.0 : R(fx - 1, fy + 1, fz - 1);
+  const double r14 = (xm || yq || zq) ? 0.0 : R(fx - 1, fy + 1, fz + 1);
+  const double r15 = (xp || ym || zm) ? 0.0 : R(fx + 1, fy - 1, fz - 1);
+  const double r16 = (xp || ym || zq) ? 0.0 : R(fx + 1, fy - 1, fz + 1);
+  const double r17 = (xp || yq || zm) ? 0.0 : R(fx + 1, fy + 1, fz - 1);
+  const double r18 = (xp || yq || zq) ? 0.0 : R(fx + 1, fy + 1, fz + 1);
+  const double r21 = (xm || ym) ? 0.0 : R(fx - 1, fy - 1, fz);
+  const double r22 = (xm || yq) ? 0.0 : R(fx - 1, fy + 1, fz);
+  const double r23 = (xp || ym) ? 0.0 : R(fx + 1, fy - 1, fz);
+  const double r24 = (xp || yq) ? 0.0 : R(fx + 1, fy + 1, fz);
+  const double r25 = (xm || zm) ? 0.0 : R(fx - 1, fy, fz - 1);
+  const double r26 = (xm || zq) ? 0.0 : R(fx - 1, fy, fz + 1);
+  const double r27 = (xp || zm) ? 0.0 : R(fx + 1, fy, fz - 1);
+  const double r28 = (xp || zq) ? 0.0 : R(fx + 1, fy, fz + 1);
+  const double r29 = (ym || zm) ? 0.0 : R(fx, fy - 1, fz - 1);
+  const double r210 = (ym || zq) ? 0.0 : R(fx, fy - 1, fz + 1);
+  const double r211 = (yq || zm) ? 0.0 : R(fx, fy + 1, fz - 1);
+  const double r212 = (yq || zq) ? 0.0 : R(fx, fy + 1, fz + 1);
+  const double r41 = zm ? 0.0 : R(fx, fy, fz - 1);
+  const double r42 = zq ? 0.0 : R(fx, fy, fz + 1);
+  const double r43 = ym ? 0.0 : R(fx, fy - 1, fz);
+  const double r44 = yq ? 0.0 : R(fx, fy + 1, fz);
+  const double r45 = xm ? 0.0 : R(fx - 1, fy, fz);
+  const double r46 = xp ? 0.0 : R(fx + 1, fy, fz);
+  const double r8 = R(fx, fy, fz);
+  const double s8 = r11 + r12 + r13 + r14 + r15 + r16 + r17 + r18;
+  const double s12 = r21 + r22 + r23 + r24 + r25 + r26 + r27 + r28 + r29 + r210 + r211 + r212;
+  const double s6 = r41 + r42 + r43 + r44 + r45 + r46;
+  return 0.125 * (s8 + 2.0 * s12 + 4.0 * s6 + 8.0 * r8);
+}
+
 }  // namespace hpc

@@ -232,25 +232,18 @@ static int pcg_u_dev(hpc_ctx* c, int l, double small_k, double Ut, int nb, int t
   m.s_out2 = S_RNORM;
   if ((rc = launch_mech(c, m))) return rc;
   for (int it = 0; it < nb; ++it) {
-    double* p_new = (it % 2 == 0) ? F.p : F.tmp3;
-    double* p_old = (it % 2 == 0) ? F.tmp3 : F.p;
+    if ((rc = launch_dir_update(c, l, 3, F.ru, F.preMu, F.p, it == 0, slot_rz(it), slot_rz(it - 1)))) return rc;
     MechCall q{};
     q.level = l;
     q.finest = m.finest;
     q.epi = EPI_PCG;
-    q.src = p_old;
+    q.src = F.p;
     q.out = F.w;
     q.small_k = small_k;
-    q.invM = F.preMu;
-    q.r = F.ru;
-    q.p_new = p_new;
-    q.first = it == 0;
-    q.s_rz = slot_rz(it);
-    q.s_rz_prev = slot_rz(it - 1);
     q.s_out0 = slot_pw(it);
     q.s_out1 = q.s_out2 = -1;
     if ((rc = launch_mech(c, q))) return rc;
-    if ((rc = launch_mech_update(c, l, p_new, slot_rz(it), slot_pw(it), slot_rz(it + 1), slot_rn(it)))) return rc;
+    if ((rc = launch_mech_update(c, l, F.p, slot_rz(it), slot_pw(it), slot_rz(it + 1), slot_rn(it)))) return rc;
   }
   return HPC_OK;
 }
@@ -273,37 +266,28 @@ static int pcg_d_dev(hpc_ctx* c, int l, double lc, int nb) {
   m.s_out2 = slot_rz(0);
   if ((rc = launch_pf(c, m))) return rc;
   for (int it = 0; it < nb; ++it) {
-    double* p_new = (it % 2 == 0) ? F.pd : F.tmp1;
-    double* p_old = (it % 2 == 0) ? F.tmp1 : F.pd;
+    if ((rc = launch_dir_update(c, l, 1, F.R, F.preMd, F.pd, it == 0, slot_rz(it), slot_rz(it - 1)))) return rc;
     PfCall q{};
     q.level = l;
     q.epi = EPI_PCG;
-    q.src = p_old;
+    q.src = F.pd;
     q.out = F.wd;
     q.lc = lc;
-    q.invM = F.preMd;
-    q.r = F.R;
-    q.p_new = p_new;
-    q.first = it == 0;
-    q.s_rz = slot_rz(it);
-    q.s_rz_prev = slot_rz(it - 1);
     q.s_out0 = slot_pw(it);
     q.s_out1 = q.s_out2 = -1;
     if ((rc = launch_pf(c, q))) return rc;
-    if ((rc = launch_pf_update(c, l, p_new, slot_rz(it), slot_pw(it), slot_rz(it + 1), slot_rn(it)))) return rc;
+    if ((rc = launch_pf_update(c, l, F.pd, slot_rz(it), slot_pw(it), slot_rz(it + 1), slot_rn(it)))) return rc;
   }
   return HPC_OK;
 }
 
-// cycle_u (mechanical_multigrid.cpp:18-54); returns smoother iterations via *iters.
-static int cycle_u_dev(hpc_ctx* c, int l, const hpc_mg& mg, double small_k, double Ut, int t, long long* iters) {
+static int cycle_u_dev(hpc_ctx* c, int l, const hpc_mg& mg, double small_k, double Ut, int t, long long* iters);
+static int cycle_d_dev(hpc_ctx* c, int l, const hpc_mg& mg, double lc, long long* iters);
+
+// The part of cycle_u(l) between its pre- and post-smoothing: coarsen_u, coarsen_fu, gamma cycles on
+// level l-1, refine_u (mechanical_multigrid.cpp:38-48).  Below the finest level t plays no role.
+static int coarse_part_u(hpc_ctx* c, int l, const hpc_mg& mg, double small_k, double Ut, int t, long long* iters) {
   int rc;
-  if (l == 0) {
-    *iters += mg.nu0;
-    return pcg_u_dev(c, 0, small_k, Ut, mg.nu0, t);
-  }
-  if ((rc = pcg_u_dev(c, l, small_k, Ut, mg.nu1, t))) return rc;
-  *iters += mg.nu1;
   if ((rc = launch_inject_u(c, l, Ut))) return rc;  // coarsen_u
   MechCall f{};                                      // coarsen_fu: fu_c = K_c u_c + FW(ru_f)
   f.level = l - 1;
@@ -318,20 +302,26 @@ static int cycle_u_dev(hpc_ctx* c, int l, const hpc_mg& mg, double small_k, doub
   if ((rc = launch_mech(c, f))) return rc;
   for (int j = 1; j <= mg.gamma; ++j)
     if ((rc = cycle_u_dev(c, l - 1, mg, small_k, Ut, t, iters))) return rc;
-  if ((rc = launch_prolong(c, l, c->F[l - 1].u, c->F[l - 1].uold, c->F[l].u, 3, true, Ut))) return rc;  // refine_u
+  return launch_prolong(c, l, c->F[l - 1].u, c->F[l - 1].uold, c->F[l].u, 3, true, Ut);  // refine_u
+}
+
+// cycle_u (mechanical_multigrid.cpp:18-54); returns smoother iterations via *iters.
+static int cycle_u_dev(hpc_ctx* c, int l, const hpc_mg& mg, double small_k, double Ut, int t, long long* iters) {
+  int rc;
+  if (l == 0) {
+    *iters += mg.nu0;
+    return pcg_u_dev(c, 0, small_k, Ut, mg.nu0, t);
+  }
+  if ((rc = pcg_u_dev(c, l, small_k, Ut, mg.nu1, t))) return rc;
+  *iters += mg.nu1;
+  if ((rc = coarse_part_u(c, l, mg, small_k, Ut, t, iters))) return rc;
   *iters += mg.nu2;
   return pcg_u_dev(c, l, small_k, Ut, mg.nu2, t);
 }
 
-// cycle_d (phase_field_multigrid.cpp:18-44), including the nu2 x nu2 post-smoothing (:41-42).
-static int cycle_d_dev(hpc_ctx* c, int l, const hpc_mg& mg, double lc, long long* iters) {
+// The part of cycle_d(l) between its pre- and post-smoothing (phase_field_multigrid.cpp:39-43).
+static int coarse_part_d(hpc_ctx* c, int l, const hpc_mg& mg, double lc, long long* iters) {
   int rc;
-  if (l == 0) {
-    *iters += mg.nu0;
-    return pcg_d_dev(c, 0, lc, mg.nu0);
-  }
-  if ((rc = pcg_d_dev(c, l, lc, mg.nu1))) return rc;
-  *iters += mg.nu1;
   if ((rc = launch_inject_d(c, l))) return rc;  // coarsen_d
   PfCall f{};                                    // coarsen_f_d
   f.level = l - 1;
@@ -345,11 +335,93 @@ static int cycle_d_dev(hpc_ctx* c, int l, const hpc_mg& mg, double lc, long long
   if ((rc = launch_pf(c, f))) return rc;
   for (int j = 1; j <= mg.gamma; ++j)
     if ((rc = cycle_d_dev(c, l - 1, mg, lc, iters))) return rc;
-  if ((rc = launch_prolong(c, l, c->F[l - 1].d, c->F[l - 1].dold, c->F[l].d, 1, false, 0.0))) return rc;  // refine_d
+  return launch_prolong(c, l, c->F[l - 1].d, c->F[l - 1].dold, c->F[l].d, 1, false, 0.0);  // refine_d
+}
+
+// cycle_d (phase_field_multigrid.cpp:18-44), including the nu2 x nu2 post-smoothing (:41-42).
+static int cycle_d_dev(hpc_ctx* c, int l, const hpc_mg& mg, double lc, long long* iters) {
+  int rc;
+  if (l == 0) {
+    *iters += mg.nu0;
+    return pcg_d_dev(c, 0, lc, mg.nu0);
+  }
+  if ((rc = pcg_d_dev(c, l, lc, mg.nu1))) return rc;
+  *iters += mg.nu1;
+  if ((rc = coarse_part_d(c, l, mg, lc, iters))) return rc;
   for (int i = 1; i <= mg.nu2; ++i) {
     if ((rc = pcg_d_dev(c, l, lc, mg.nu2))) return rc;
     *iters += mg.nu2;
   }
+  return HPC_OK;
+}
+
+// ---------------------------------------------------------------- graph replay of coarse parts
+static bool same_mg(const hpc_mg& a, const hpc_mg& b) {
+  return a.nu0 == b.nu0 && a.nu1 == b.nu1 && a.nu2 == b.nu2 && a.gamma == b.gamma;
+}
+
+// Runs `body` (a coarse part) through a cached CUDA graph: captured on the first call whose
+// parameters differ from the cached ones (the kernels' first use must already have happened,
+// `allow_capture`), replayed afterwards.  Kernel launches are counted per replay.
+template <class Body>
+static int run_graphed(hpc_ctx* c, hpc_ctx::CoarseGraph& g, const hpc_mg& mg, double a, double b, bool allow_capture,
+                       Body body) {
+  const bool hit = g.valid && same_mg(g.mg, mg) && g.a == a && g.b == b;
+  if (!c->use_graphs || (!hit && !allow_capture)) return body();
+  if (!hit) {
+    if (g.valid) {
+      cudaGraphExecDestroy(g.exec);
+      g.valid = 0;
+    }
+    HPC_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const long long k0 = c->launches;
+    const int rc = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate");
+    g.kernels = c->launches - k0;
+    c->launches = k0;
+    g.valid = 1;
+    g.mg = mg;
+    g.a = a;
+    g.b = b;
+  }
+  HPC_CUDA(cudaGraphLaunch(g.exec, c->stream));
+  c->launches += g.kernels;
+  return HPC_OK;
+}
+
+// Top-level cycles of the solves: the finest level's smoothing is launched directly (its kernels
+// are large and individually timed), everything below it is replayed as one graph.
+static int cycle_u_top(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, bool allow_capture) {
+  const int L = c->maxlevel;
+  long long it = 0;
+  if (L == 0) return cycle_u_dev(c, 0, mg, small_k, Ut, t, &it);
+  int rc;
+  if ((rc = pcg_u_dev(c, L, small_k, Ut, mg.nu1, t))) return rc;
+  if ((rc = run_graphed(c, c->gmech, mg, small_k, Ut, allow_capture,
+                        [&] { return coarse_part_u(c, L, mg, small_k, Ut, t, &it); })))
+    return rc;
+  return pcg_u_dev(c, L, small_k, Ut, mg.nu2, t);
+}
+
+static int cycle_d_top(hpc_ctx* c, const hpc_mg& mg, double lc, bool allow_capture) {
+  const int L = c->maxlevel;
+  long long it = 0;
+  if (L == 0) return cycle_d_dev(c, 0, mg, lc, &it);
+  int rc;
+  if ((rc = pcg_d_dev(c, L, lc, mg.nu1))) return rc;
+  if ((rc = run_graphed(c, c->gpf, mg, lc, 0.0, allow_capture, [&] { return coarse_part_d(c, L, mg, lc, &it); })))
+    return rc;
+  for (int i = 1; i <= mg.nu2; ++i)
+    if ((rc = pcg_d_dev(c, L, lc, mg.nu2))) return rc;
   return HPC_OK;
 }
 
@@ -398,8 +470,7 @@ static int u_entire_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut,
   const int per_cycle = (L == 0) ? mg.nu0 : mg.nu1 + mg.nu2;
   for (int j = 1; j <= mg.ncy; ++j) {
     if (rel > mech_tol) {
-      long long it = 0;
-      if ((rc = cycle_u_dev(c, L, mg, small_k, Ut, t, &it))) return rc;
+      if ((rc = cycle_u_top(c, mg, small_k, Ut, t, *cycles > 0))) return rc;
       ++*cycles;
       *fin_iters += per_cycle;
       if ((rc = launch_dot(c, L, 3, c->F[L].ru, nullptr, S_RNORM))) return rc;
@@ -451,8 +522,7 @@ static int phase_field_dev(hpc_ctx* c, const hpc_mg& mg, double lc, double pf_to
   for (int j = 1; j <= mg.ncy; ++j) {
     if (r_norm > pf_tol) {
       if (sres > pf_tol) {
-        long long it = 0;
-        if ((rc = cycle_d_dev(c, L, mg, lc, &it))) return rc;
+        if ((rc = cycle_d_top(c, mg, lc, *cycles > 0))) return rc;
         ++*cycles;
         *fin_iters += per_cycle;
       }
@@ -523,6 +593,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   c->maxlevel = geo->maxlevel;
   c->device = device;
   c->choice_quirk = 1;
+  c->use_graphs = 1;
   c->timing_class = HPC_KC_NONE;
   HostLevel lv[kMaxLevels];
   host_geometry(*geo, c->box, lv);
@@ -639,6 +710,8 @@ int hpc_destroy(hpc_ctx* c) {
   if (c->hscal) cudaFreeHost(c->hscal);
   for (int i = 0; i < 2 * c->tev_cap; ++i) cudaEventDestroy(c->tev[i]);
   delete[] c->tev;
+  if (c->gmech.valid) cudaGraphExecDestroy(c->gmech.exec);
+  if (c->gpf.valid) cudaGraphExecDestroy(c->gpf.exec);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return HPC_OK;

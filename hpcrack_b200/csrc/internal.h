@@ -78,6 +78,16 @@ struct hpc_ctx {
   void* bc_dev_base;     // one allocation for all axis flags
   long long launches;
   int choice_quirk;
+  // CUDA graphs of the coarse part of a V-cycle (everything below the finest level), cached with
+  // the parameters they were captured for
+  struct CoarseGraph {
+    cudaGraphExec_t exec;
+    long long kernels;
+    int valid;
+    hpc_mg mg;
+    double a, b;  // small_k, Ut (mechanical) or lc (phase field)
+  } gmech, gpf;
+  int use_graphs;
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
@@ -163,6 +173,9 @@ int launch_pf_diag(hpc_ctx* c, int level, double lc, double* out);
 // nodes; scal[s_rz_next] = sum r^2/preM; scal[s_rn] = sum r^2.
 int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
 int launch_pf_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
+// p = r M^-1 + beta p (beta = scal[s_rz]/scal[s_rz_prev], 0 if first), in place
+int launch_dir_update(hpc_ctx* c, int level, int ncomp, const double* r, const double* invM, double* p, bool first,
+                      int s_rz, int s_rz_prev);
 // Dirichlet operations on a 3n vector of a level: kind 0 set u (Ut on top), 1 copy src into v,
 // 2 zero v.
 int launch_bc(hpc_ctx* c, int level, double* v, const double* src, int kind, double Ut);

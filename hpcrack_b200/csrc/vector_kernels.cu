@@ -35,10 +35,6 @@ int row_grid(const LevelGeo& g, int per_sm = 8) {
   for (long long row = blockIdx.x; row < (long long)(g).ny * (g).nz; row += gridDim.x) \
     for (int i = threadIdx.x, j = (int)(row % (g).ny), kz = (int)(row / (g).ny); i < (g).nx; i += blockDim.x)
 
-__device__ __forceinline__ long long nidx(const LevelGeo& g, int i, int j, int k) {
-  return (long long)i + (long long)j * g.px + (long long)k * g.plane;
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------------------------
@@ -100,6 +96,29 @@ int launch_pf_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw,
   const LevelFields& F = c->F[level];
   pf_update_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, F.d, F.R, p, F.wd, F.preMd, s_rz, s_pw,
                                                               make_red(c, s_rz_next, s_rn, -1));
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+
+// PCG direction (mechanical_pcg.cpp:274-292, phase_field_pcg.cpp:178-186):
+// z = r M^-1, beta = rz/rz_old (0 on a call's first iteration), p = z + beta p, in place.
+__global__ void dir_update_kernel(LevelGeo g, int ncomp, const double* r, const double* invM, double* p, int first,
+                                  const double* scal, int s_rz, int s_rz_prev) {
+  const double beta = first ? 0.0 : scal[s_rz] / scal[s_rz_prev];
+  FOR_NODES(g) {
+    const long long n = nidx(g, i, j, kz);
+    for (int m = 0; m < ncomp; ++m) {
+      const long long o = n + (long long)m * g.n;
+      const double z = r[o] * invM[o];
+      p[o] = first ? z : fma(beta, p[o], z);
+    }
+  }
+}
+int launch_dir_update(hpc_ctx* c, int level, int ncomp, const double* r, const double* invM, double* p, bool first,
+                      int s_rz, int s_rz_prev) {
+  const LevelGeo& g = c->L[level];
+  dir_update_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, ncomp, r, invM, p, first ? 1 : 0, c->scal, s_rz,
+                                                               s_rz_prev);
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
 }
@@ -254,44 +273,7 @@ int launch_inject_d(hpc_ctx* c, int lf) {
   return HPC_OK;
 }
 
-// coarsen_f_standard_routine (:124-342), standalone form.
-__device__ __forceinline__ double full_weight(const LevelGeo& gf, const double* rf, int fx, int fy, int fz) {
-  const int Xl = gf.nx - 2, Yl = gf.ny - 2, Zl = gf.nz - 2;
-  auto R = [&](int a, int b, int c) -> double { return rf[nidx(gf, a, b, c)]; };
-  const bool xm = fx < 1, xp = fx > Xl, ym = fy < 1, yq = fy > Yl, zm = fz < 1, zq = fz > Zl;
-  const double r11 = (xm || ym || zm) ? 0.0 : R(fx - 1, fy - 1, fz - 1);
-  const double r12 = (xm || ym || zq) ? 0.0 : R(fx - 1, fy - 1, fz + 1);
-  const double r13 = (xm || yq || zm) ? 0.0 : R(fx - 1, fy + 1, fz - 1);
-  const double r14 = (xm || yq || zq) ? 0.0 : R(fx - 1, fy + 1, fz + 1);
-  const double r15 = (xp || ym || zm) ? 0.0 : R(fx + 1, fy - 1, fz - 1);
-  const double r16 = (xp || ym || zq) ? 0.0 : R(fx + 1, fy - 1, fz + 1);
-  const double r17 = (xp || yq || zm) ? 0.0 : R(fx + 1, fy + 1, fz - 1);
-  const double r18 = (xp || yq || zq) ? 0.0 : R(fx + 1, fy + 1, fz + 1);
-  const double r21 = (xm || ym) ? 0.0 : R(fx - 1, fy - 1, fz);
-  const double r22 = (xm || yq) ? 0.0 : R(fx - 1, fy + 1, fz);
-  const double r23 = (xp || ym) ? 0.0 : R(fx + 1, fy - 1, fz);
-  const double r24 = (xp || yq) ? 0.0 : R(fx + 1, fy + 1, fz);
-  const double r25 = (xm || zm) ? 0.0 : R(fx - 1, fy, fz - 1);
-  const double r26 = (xm || zq) ? 0.0 : R(fx - 1, fy, fz + 1);
-  const double r27 = (xp || zm) ? 0.0 : R(fx + 1, fy, fz - 1);
-  const double r28 = (xp || zq) ? 0.0 : R(fx + 1, fy, fz + 1);
-  const double r29 = (ym || zm) ? 0.0 : R(fx, fy - 1, fz - 1);
-  const double r210 = (ym || zq) ? 0.0 : R(fx, fy - 1, fz + 1);
-  const double r211 = (yq || zm) ? 0.0 : R(fx, fy + 1, fz - 1);
-  const double r212 = (yq || zq) ? 0.0 : R(fx, fy + 1, fz + 1);
-  const double r41 = zm ? 0.0 : R(fx, fy, fz - 1);
-  const double r42 = zq ? 0.0 : R(fx, fy, fz + 1);
-  const double r43 = ym ? 0.0 : R(fx, fy - 1, fz);
-  const double r44 = yq ? 0.0 : R(fx, fy + 1, fz);
-  const double r45 = xm ? 0.0 : R(fx - 1, fy, fz);
-  const double r46 = xp ? 0.0 : R(fx + 1, fy, fz);
-  const double r8 = R(fx, fy, fz);
-  const double s8 = r11 + r12 + r13 + r14 + r15 + r16 + r17 + r18;
-  const double s12 = r21 + r22 + r23 + r24 + r25 + r26 + r27 + r28 + r29 + r210 + r211 + r212;
-  const double s6 = r41 + r42 + r43 + r44 + r45 + r46;
-  return 0.125 * (s8 + 2.0 * s12 + 4.0 * s6 + 8.0 * r8);
-}
-
+// coarsen_f_standard_routine (:124-342), standalone form (full_weight in device_common.cuh).
 __global__ void restrict_kernel(LevelGeo gc, LevelGeo gf, const double* rf, const double* Fic, double* fc, int ncomp) {
   FOR_NODES(gc) {
     const long long nc = nidx(gc, i, j, kz);
