@@ -101,6 +101,7 @@ SIGNATURES = {
     "hpc_coarsen_f_standard": [_ctx, _i, _i, _i, _i, _i],
     "hpc_refine_standard": [_ctx, _i, _i, _i, _i, _i],
     "hpc_image_material": [_ctx, C.POINTER(C.c_uint8), _ip, _i, _ip, _dp, _dp, _dp, _d],
+    "hpc_dmax_noalloc": [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p],
 }
 _RESTYPE = {"hpc_last_error": C.c_char_p, "hpc_stream": C.c_void_p}
 

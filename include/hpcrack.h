@@ -212,6 +212,18 @@ int hpc_refine_standard(hpc_ctx* ctx, int uf_field, int uc_field, int ucold_fiel
 int hpc_image_material(hpc_ctx* ctx, const uint8_t* image, const int* voxel_n, int ngray, const int* gray,
                        const double* E, const double* nu, const double* gc, double voxel_size);
 
+/* ---------------- allocation-free variant ---------------- */
+/* No counterpart in the reference: d_max and delta_d_max (the reductions of hpc_d_max /
+ * hpc_delta_d_max) of caller-owned DEVICE arrays d and d_old of n doubles, written to the caller's
+ * device array out[2] = {max(0, max(d - d_old)), max(0, max d)}, on `stream` (a cudaStream_t, may
+ * be null).  For callers that cannot allocate device memory (an allocator that owns the device,
+ * code that must not trigger cudaMalloc's implicit synchronisation): the block partials live in a
+ * fixed 1 MiB __device__ array that every device loading the library keeps until exit, so the call
+ * allocates nothing.  n is limited to 134217728 (HPC_ERR_ARG beyond).  The first call on a device
+ * looks up the scratch address once.  All calls share the scratch: calls that overlap on the GPU
+ * race. */
+int hpc_dmax_noalloc(const double* d, const double* d_old, long long n, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
