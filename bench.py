@@ -33,6 +33,10 @@ if ROOT not in sys.path:
 METRIC = "MDoF-iter/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+PCG_APPLY_BYTES_PER_NODE = 73
+# DRAM bytes (read + write) per launch of the finest PCG apply, from one ncu capture per workload
+# (None until captured); a 257^3 figure is the 193^3 capture scaled by the node count.
+PCG_APPLY_TRAFFIC = {}
 
 
 def parse_args():
@@ -48,7 +52,58 @@ def parse_args():
     ap.add_argument("--kernel-only", type=int, default=0, metavar="NB",
                     help="profiling driver: set the specimen up, run one finest-level pcg_u with NB iterations "
                          "(NB launches of the dominant kernel) and exit")
+    ap.add_argument("--profile-cycles", type=int, default=0, metavar="K",
+                    help="profiling driver: set the specimen up and run two increments capped at K mechanical "
+                         "and K phase-field V-cycles each (the step's kernel mix in a bounded launch count)")
+    ap.add_argument("--serve", type=float, default=0.0, metavar="RATE",
+                    help="serving form: Poisson arrivals at RATE requests/s (seed 7) through the continuous-"
+                         "admission server; prints solves/s and p50/p99 latency")
+    ap.add_argument("--batch", type=int, default=0, metavar="N",
+                    help="batched form: N specimens of the uneven-size mix (seeds 100..) submitted at once")
+    ap.add_argument("--requests", type=int, default=24, help="requests in a --serve sample")
+    ap.add_argument("--increments", type=int, default=0, help="increments per request (default 10 serve, 5 batch)")
+    ap.add_argument("--slots", type=int, default=8, help="concurrent requests on the GPU")
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
+    ap.add_argument("--sizes", default="", help="serve: comma list of cubic sizes to draw from (default: the mix)")
     return ap.parse_args()
+
+
+def run_serving(args, local):
+    """Serving / batched forms: whole fracture runs through hpcrack_b200.serving.SolveServer."""
+    import torch
+    from hpcrack_b200 import serving as sv
+    torch.cuda.set_device(local)
+    budget = int(args.hbm_budget_gb * (1 << 30))
+    if args.batch:
+        inc = args.increments or 5
+        reqs = [sv.Request(i, sv.batch_specimen(100 + i, inc), inc) for i in range(args.batch)]
+        metric, form = "solves/s", f"batched: {args.batch} specimens (seeds 100..{99 + args.batch}), sizes per axis " \
+                                   f"from {{33,65,97,129,161}}, {inc} increments each, submitted at t=0"
+    else:
+        inc = args.increments or 10
+        kw = {}
+        if args.sizes:
+            kw = {"sizes": tuple((int(n),) * 3 for n in args.sizes.split(",")), "weights": None}
+            kw["weights"] = tuple(1.0 for _ in kw["sizes"])
+        reqs = sv.serve_mix(args.requests, args.serve, seed=7, increments=inc, **kw)
+        metric, form = "solves/s", f"served: {args.requests} requests, Poisson arrivals at {args.serve}/s (seed 7), " \
+                                   f"{inc} increments each"
+    srv = sv.SolveServer(budget, args.slots, solver_factory=sv.default_factory(local))
+    t0 = time.perf_counter()
+    res = srv.replay(reqs)
+    wall = time.perf_counter() - t0
+    st = sv.latency_stats(res, wall)
+    dof_iters = 0.0
+    for r, q in zip(res, reqs):
+        nx, ny, nz = q.workload.nodes
+        dof_iters += sum(3.0 * nx * ny * nz * o[6] + nx * ny * nz * o[7] for o in r.outputs)
+    line = {"metric": metric, "value": st["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic", "config": {"workload": form, "slots": args.slots,
+                                                            "hbm_budget_gb": args.hbm_budget_gb},
+            "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "wall_s": wall,
+            "mdof_iter_per_s": dof_iters / wall / 1e6, "peak_active": srv.peak_active,
+            "peak_hbm_gb": srv.peak_used / (1 << 30)}
+    print(json.dumps(line), flush=True)
 
 
 def run_kernel_only(args, local):
@@ -61,6 +116,23 @@ def run_kernel_only(args, local):
     _, fn = hier.pcg_u(w.maxlevel, w.small_k, 1.0, args.kernel_only, 0, 0.0)
     hier.sync()
     print(json.dumps({"kernel_only": args.kernel_only, "workload": w.name, "f_norm": fn}), flush=True)
+    hier.close()
+
+
+def run_profile_cycles(args, local):
+    """A short, bounded program for profilers: two increments whose V-cycle counts are capped at K."""
+    from hpcrack_b200 import microstructure as ms
+    w = ms.make_workload(args.workload)
+    hier = load_specimen(w, local)
+    K = args.profile_cycles
+    mg_u = tuple(w.mg_u[:4]) + (K,)
+    mg_d = tuple(w.mg_d[:4]) + (K,)
+    launches0 = hier.launch_count()
+    outs = [hier.step(t, mg_u, mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du, dU_factor=w.du_factor,
+                      mech_tol=w.mech_tol, pf_tol=w.pf_tol) for t in range(2)]
+    hier.sync()
+    print(json.dumps({"profile_cycles": K, "workload": w.name, "launches": hier.launch_count() - launches0,
+                      "mech_cycles": [int(o[4]) for o in outs], "pf_cycles": [int(o[5]) for o in outs]}), flush=True)
     hier.close()
 
 
@@ -295,20 +367,18 @@ def run_b200(args, rank, world, local):
     max_ms, tot_dof_iters = replicas.aggregate(ms_total, dof_iters, world)
     value = tot_dof_iters / (max_ms / 1e3) / 1e6
 
-    # roofline of the dominant kernel: fused direction update + K(d) p + (p, w) on the finest level.
-    # Algorithmic bytes per finest node: r, preM, p_old, p_new, w (3 x 8 B each), bulK, G, d (8 B each),
-    # regime (1 B) = 145 B; the first iteration of each smoother call does not read p_old (121 B).
+    # roofline of the dominant kernel: the finest-level PCG apply w = K(d) p with the (p, w) reduction.
+    # Algorithmic bytes per finest node: p read and w written (3 x 8 B each), bulK, G, d read (8 B each),
+    # regime byte read = 73 B.
     roofline = None
     if kn > 0:
-        firsts = 2 * mech_cycles if w.maxlevel >= 1 else mech_cycles
-        firsts = min(firsts, kn)
-        bytes_total = N * (145.0 * (kn - firsts) + 121.0 * firsts)
+        bytes_total = N * PCG_APPLY_BYTES_PER_NODE * kn
         achieved = bytes_total / (kms / 1e3) / 1e9
         peak, src = peaks()
-        roofline = {"bound": "hbm", "kernel": "mech_kernel<finest, PCG> (fused z/p update + K(d)p + pw)",
+        roofline = {"bound": "hbm", "kernel": "mech_kernel<finest, PCG> (w = K(d) p, (p, w))",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "peak_source": src, "traffic": None, "launches": kn, "avg_launch_ms": kms / kn,
-                    "bytes_per_node": [145, 121]}
+                    "peak_source": src, "traffic": PCG_APPLY_TRAFFIC.get(w.name), "launches": kn,
+                    "avg_launch_ms": kms / kn, "bytes_per_node": PCG_APPLY_BYTES_PER_NODE}
 
     # ------------------------------------------------------------ end to end through the C ABI
     e2e = None
@@ -379,6 +449,10 @@ def main():
     try:
         if args.kernel_only:
             run_kernel_only(args, local)
+        elif args.profile_cycles:
+            run_profile_cycles(args, local)
+        elif args.serve or args.batch:
+            run_serving(args, local)
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

@@ -2,8 +2,10 @@
 // fused epilogues (residual, (p, K p), FAS right-hand side, reactions).
 //
 // Tiling ("warp strip"): a warp owns a strip of 32 node columns in x (31 elements, 30 output
-// nodes), kWY element rows in y (kWY-1 output node rows) and kCZ output node planes in z, and
-// streams it row by row, layer by layer.  Node rows are staged into a per-warp shared-memory ring
+// nodes), wy element rows in y (wy-1 output node rows) and cz output node planes in z, and
+// streams it row by row, layer by layer.  The strip shape (wy, cz) is chosen per level: long strips
+// on large levels (little recomputation at strip edges), short ones on small levels, where the
+// serial chain of elements a warp computes would otherwise set the kernel's duration.  Node rows are staged into a per-warp shared-memory ring
 // with cp.async two rows ahead of use, so global-memory latency never sits on the element math.
 // Per row step a lane computes one element from the staged rows; x-neighbour contributions are
 // combined with one shuffle, y-neighbours through registers (the previous row's upper-face sums)
@@ -21,23 +23,37 @@
 namespace hpc {
 
 constexpr int kWarps = 4;    // warps per block
-constexpr int kWY = 8;       // element rows per strip (kWY - 1 output node rows)
-constexpr int kCZ = 16;      // output planes per strip
+constexpr int kWY = 8;       // largest strip height in element rows (wy - 1 output node rows)
 constexpr int kOX = 30;      // output nodes per strip in x (lanes 1..30)
 constexpr int kRowW = 33;    // staged row width (32 lanes + the x+1 read of lane 31)
 constexpr int kRing = 4;     // staged node rows in flight / in use per warp
 
 struct StripGeo {
   int tx, ty, tz;            // strips per axis
+  int wy, cz;                // element rows (2..kWY) and output planes per strip
   long long nstrips;
 };
 
-__host__ __device__ inline StripGeo strip_geo(const LevelGeo& g) {
+inline StripGeo strip_geo(const LevelGeo& g, int wy, int cz) {
   StripGeo s;
+  s.wy = wy;
+  s.cz = cz;
   s.tx = (g.nx + kOX - 1) / kOX;
-  s.ty = (g.ny + kWY - 2) / (kWY - 1);
-  s.tz = (g.nz + kCZ - 1) / kCZ;
+  s.ty = (g.ny + wy - 2) / (wy - 1);
+  s.tz = (g.nz + cz - 1) / cz;
   s.nstrips = (long long)s.tx * s.ty * s.tz;
+  return s;
+}
+
+// The longest strip shape that still gives every resident warp slot about two strips; small
+// levels end at 2 x 2 (one output row, two output planes per warp).
+inline StripGeo choose_strips(const LevelGeo& g, long long warp_slots) {
+  static const int shapes[][2] = {{8, 16}, {8, 8}, {4, 8}, {4, 4}, {2, 4}, {2, 2}};
+  StripGeo s{};
+  for (const auto& sh : shapes) {
+    s = strip_geo(g, sh[0], sh[1]);
+    if (s.nstrips >= 2 * warp_slots) break;
+  }
   return s;
 }
 
@@ -52,19 +68,19 @@ __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::: "memory"); }
 
-// A strip's staged stream: for each layer kk = z0-1 .. zend, node rows y = y0-1 .. y0-1+kWY
-// (kWY+1 rows), each row holding NF fields on the two planes kk and kk+1.  Stream row s sits in
+// A strip's staged stream: for each layer kk = z0-1 .. zend, node rows y = y0-1 .. y0-1+wy
+// (rows = wy+1 rows), each row holding NF fields on the two planes kk and kk+1.  Stream row s sits in
 // ring slot s % kRing at ring[((slot*NF + f)*2 + c)*kRowW + lane].
 template <int NF>
 struct Stream {
   double* ring;
   const double* const* fields;  // NF global arrays (node-indexed)
-  int x, y0, z0, nlayers, total;
+  int x, y0, z0, nlayers, total, rows;
   const LevelGeo* g;
 
   __device__ __forceinline__ void issue(int s, int lane) {
     if (s < total) {
-      const int li = s / (kWY + 1), r = s - li * (kWY + 1);
+      const int li = s / rows, r = s - li * rows;
       const int kk = z0 - 1 + li, y = y0 - 1 + r;
       const int slot = s & (kRing - 1);
 #pragma unroll
@@ -149,11 +165,12 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
     const long long rest = strip / k.sg.tx;
     const int sy = (int)(rest % k.sg.ty);
     const int sz = (int)(rest / k.sg.ty);
-    const int x0 = sx * kOX, y0 = sy * (kWY - 1), z0 = sz * kCZ;
+    const int wy = k.sg.wy, rows = wy + 1;
+    const int x0 = sx * kOX, y0 = sy * (wy - 1), z0 = sz * k.sg.cz;
     const int x = x0 - 1 + lane;
-    const int zend = min(z0 + kCZ - 1, k.g.nz - 1);
-    Stream<NF> st{ring, fptr, x, y0, z0, zend - z0 + 2, 0, &k.g};
-    st.total = st.nlayers * (kWY + 1);
+    const int zend = min(z0 + k.sg.cz - 1, k.g.nz - 1);
+    Stream<NF> st{ring, fptr, x, y0, z0, zend - z0 + 2, 0, rows, &k.g};
+    st.total = st.nlayers * rows;
     st.issue(0, lane);
     st.issue(1, lane);
     double yp[2][3];
@@ -161,7 +178,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
       st.issue(si + 2, lane);
       cp_async_wait2();
       __syncwarp();
-      const int li = si / (kWY + 1), r = si - li * (kWY + 1);
+      const int li = si / rows, r = si - li * rows;
       const int kk = z0 - 1 + li;
       if (r == 0) {
 #pragma unroll
@@ -349,15 +366,17 @@ static int kernel_cfg(Kern kern, size_t smem, int* per_sm_out) {
   return HPC_OK;
 }
 
-// Launches a strip kernel with the occupancy the device allows (persistent grid).
+// Launches a strip kernel with the occupancy the device allows (persistent grid), choosing the
+// strip shape of the level from the number of resident warp slots.
 template <class Kern, class Args>
-static int launch_strips(hpc_ctx* c, Kern kern, const Args& a, const StripGeo& sg, size_t smem, int cls) {
-  static_assert(sizeof(Args) > 0, "");
+static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls) {
   int per_sm = 1;
   const int rc = kernel_cfg(kern, smem, &per_sm);
   if (rc) return rc;
-  const long long need = (sg.nstrips + kWarps - 1) / kWarps;
   const long long cap = (long long)num_sms() * per_sm;
+  a.sg = choose_strips(a.g, cap * kWarps);
+  const StripGeo& sg = a.sg;
+  const long long need = (sg.nstrips + kWarps - 1) / kWarps;
   const int grid = (int)(need < cap ? need : cap);
   if (grid <= 0) return HPC_OK;
   if ((size_t)grid * 3 > c->partials_cap) return cuda_fail(cudaErrorInvalidValue, "partials buffer");
@@ -373,7 +392,7 @@ static int run_mech(hpc_ctx* c, const MechK& k) {
   constexpr int NF = (D ? 0 : 3) + (F ? 3 : 2);
   const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(double);
   const int cls = (F && E == EPI_PCG && !D) ? HPC_KC_MECH_PCG_FINEST : HPC_KC_NONE;
-  return launch_strips(c, mech_kernel<F, E, D>, k, k.sg, smem, cls);
+  return launch_strips(c, mech_kernel<F, E, D>, k, smem, cls);
 }
 
 static void mech_fields(hpc_ctx* c, int level, bool finest, bool diag, const double* src, MechK& k) {
@@ -397,7 +416,6 @@ int launch_mech(hpc_ctx* c, const MechCall& m) {
   MechK k{};
   k.g = c->L[m.level];
   if (m.epi == EPI_FAS) k.gf = c->L[m.fine_level];
-  k.sg = strip_geo(k.g);
   mech_fields(c, m.level, m.finest, false, m.src, k);
   k.out = m.out;
   k.choice = c->F[m.level].choice;
@@ -423,7 +441,6 @@ int launch_mech(hpc_ctx* c, const MechCall& m) {
 int launch_mech_diag(hpc_ctx* c, int level, bool finest, double small_k, double* out) {
   MechK k{};
   k.g = c->L[level];
-  k.sg = strip_geo(k.g);
   mech_fields(c, level, finest, true, nullptr, k);
   k.choice = c->F[level].choice;
   k.small_k = small_k;
@@ -465,11 +482,12 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
     const long long rest = strip / k.sg.tx;
     const int sy = (int)(rest % k.sg.ty);
     const int sz = (int)(rest / k.sg.ty);
-    const int x0 = sx * kOX, y0 = sy * (kWY - 1), z0 = sz * kCZ;
+    const int wy = k.sg.wy, rows = wy + 1;
+    const int x0 = sx * kOX, y0 = sy * (wy - 1), z0 = sz * k.sg.cz;
     const int x = x0 - 1 + lane;
-    const int zend = min(z0 + kCZ - 1, k.g.nz - 1);
-    Stream<NF> st{ring, fptr, x, y0, z0, zend - z0 + 2, 0, &k.g};
-    st.total = st.nlayers * (kWY + 1);
+    const int zend = min(z0 + k.sg.cz - 1, k.g.nz - 1);
+    Stream<NF> st{ring, fptr, x, y0, z0, zend - z0 + 2, 0, rows, &k.g};
+    st.total = st.nlayers * rows;
     st.issue(0, lane);
     st.issue(1, lane);
     double yp[2] = {0.0, 0.0};
@@ -477,7 +495,7 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
       st.issue(si + 2, lane);
       cp_async_wait2();
       __syncwarp();
-      const int li = si / (kWY + 1), r = si - li * (kWY + 1);
+      const int li = si / rows, r = si - li * rows;
       const int kk = z0 - 1 + li;
       if (r == 0) {
         yp[0] = yp[1] = 0.0;
@@ -563,14 +581,13 @@ template <int E, bool D>
 static int run_pf(hpc_ctx* c, const PfK& k, bool finest) {
   const size_t smem = (size_t)kWarps * (kRing * 3 * 2 * kRowW + (kWY - 1) * 32) * sizeof(double);
   const int cls = (finest && E == EPI_PCG && !D) ? HPC_KC_PF_PCG_FINEST : HPC_KC_NONE;
-  return launch_strips(c, pf_kernel<E, D>, k, k.sg, smem, cls);
+  return launch_strips(c, pf_kernel<E, D>, k, smem, cls);
 }
 
 int launch_pf(hpc_ctx* c, const PfCall& p) {
   PfK k{};
   k.g = c->L[p.level];
   if (p.epi == EPI_FAS) k.gf = c->L[p.fine_level];
-  k.sg = strip_geo(k.g);
   k.fields[0] = p.src;
   k.fields[1] = c->F[p.level].gc;
   k.fields[2] = c->F[p.level].H;
@@ -593,7 +610,6 @@ int launch_pf(hpc_ctx* c, const PfCall& p) {
 int launch_pf_diag(hpc_ctx* c, int level, double lc, double* out) {
   PfK k{};
   k.g = c->L[level];
-  k.sg = strip_geo(k.g);
   k.fields[0] = c->F[level].d;
   k.fields[1] = c->F[level].gc;
   k.fields[2] = c->F[level].H;

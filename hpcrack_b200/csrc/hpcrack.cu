@@ -94,6 +94,10 @@ static bool geometry_ok(const hpc_geometry* g) {
   // finest node count per axis must stay a sane int
   for (int a = 0; a < 3; ++a)
     if ((double)g->element_nb[a] * std::pow(2.0, g->maxlevel) > 65000.0) return false;
+  // node-parallel kernels index a level with 32-bit arithmetic: padded node count below 2^31
+  double nodes = 1.0;
+  for (int a = 0; a < 3; ++a) nodes *= (double)g->element_nb[a] * std::pow(2.0, g->maxlevel) + 1.0 + (a == 0 ? 3 : 0);
+  if (nodes >= 2147483648.0) return false;
   return true;
 }
 
@@ -712,6 +716,12 @@ int hpc_destroy(hpc_ctx* c) {
   delete[] c->tev;
   if (c->gmech.valid) cudaGraphExecDestroy(c->gmech.exec);
   if (c->gpf.valid) cudaGraphExecDestroy(c->gpf.exec);
+  if (c->ck.stream) cudaStreamSynchronize(c->ck.stream);
+  if (c->ck.dev) cudaFree(c->ck.dev);
+  if (c->ck.host) cudaFreeHost(c->ck.host);
+  if (c->ck.snap) cudaEventDestroy(c->ck.snap);
+  if (c->ck.done) cudaEventDestroy(c->ck.done);
+  if (c->ck.stream) cudaStreamDestroy(c->ck.stream);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return HPC_OK;
@@ -828,6 +838,79 @@ int hpc_set_state(hpc_ctx* c, const double* s6) {
   if (!c || !s6) return arg_fail("null argument");
   c->f_norm = s6[0]; c->fd_norm = s6[1]; c->Ue = s6[2]; c->Ut = s6[3]; c->dU = s6[4]; c->uprop = s6[5];
   return HPC_OK;
+}
+
+// ---------------------------------------------------------------- checkpoint / restart
+// The staggered loop's whole state between two increments is the finest u (3 components), H, d,
+// d_old and the six loop scalars: every coarse field, the regimes and the right-hand sides are
+// rebuilt from them by the next increment (crack_propagation.cpp:65-121).
+static double* ck_source(hpc_ctx* c, int i) {
+  const int L = c->maxlevel;
+  switch (i) {
+    case 0: case 1: case 2: return c->F[L].u + (long long)i * c->L[L].n;
+    case 3: return c->F[L].H;
+    case 4: return c->F[L].d;
+    default: return c->d_old;
+  }
+}
+
+int hpc_checkpoint_begin(hpc_ctx* c, int t) {
+  if (!c) return arg_fail("null context");
+  HPC_CUDA(cudaSetDevice(c->device));
+  const LevelGeo& g = c->L[c->maxlevel];
+  const size_t dense = (size_t)g.nx * g.ny * g.nz;
+  hpc_ctx::Checkpoint& k = c->ck;
+  if (!k.dev) {  // first checkpoint of this context: buffers, copy stream and events
+    HPC_CUDA(cudaMalloc((void**)&k.dev, 6 * dense * sizeof(double)));
+    HPC_CUDA(cudaMallocHost((void**)&k.host, 6 * dense * sizeof(double)));
+    HPC_CUDA(cudaStreamCreateWithFlags(&k.stream, cudaStreamNonBlocking));
+    HPC_CUDA(cudaEventCreateWithFlags(&k.snap, cudaEventDisableTiming));
+    HPC_CUDA(cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming));
+  }
+  // the previous copy must have left the snapshot before it is overwritten
+  if (k.pending) HPC_CUDA(cudaStreamWaitEvent(c->stream, k.done, 0));
+  for (int i = 0; i < 6; ++i)
+    HPC_CUDA(cudaMemcpy2DAsync(k.dev + i * dense, sizeof(double) * g.nx, ck_source(c, i), sizeof(double) * g.px,
+                               sizeof(double) * g.nx, (size_t)g.ny * g.nz, cudaMemcpyDeviceToDevice, c->stream));
+  HPC_CUDA(cudaEventRecord(k.snap, c->stream));
+  HPC_CUDA(cudaStreamWaitEvent(k.stream, k.snap, 0));
+  HPC_CUDA(cudaMemcpyAsync(k.host, k.dev, 6 * dense * sizeof(double), cudaMemcpyDeviceToHost, k.stream));
+  HPC_CUDA(cudaEventRecord(k.done, k.stream));
+  k.t = t;
+  k.pending = 1;
+  k.valid = 1;
+  k.state[0] = c->f_norm; k.state[1] = c->fd_norm; k.state[2] = c->Ue;
+  k.state[3] = c->Ut; k.state[4] = c->dU; k.state[5] = c->uprop;
+  return HPC_OK;
+}
+
+int hpc_checkpoint_wait(hpc_ctx* c, int* t, const double** fields, double* state6) {
+  if (!c) return arg_fail("null context");
+  hpc_ctx::Checkpoint& k = c->ck;
+  if (!k.valid) return arg_fail("no checkpoint has been started");
+  HPC_CUDA(cudaSetDevice(c->device));
+  if (k.pending) {
+    HPC_CUDA(cudaEventSynchronize(k.done));
+    k.pending = 0;
+  }
+  if (t) *t = k.t;
+  if (fields) *fields = k.host;
+  if (state6)
+    for (int i = 0; i < 6; ++i) state6[i] = k.state[i];
+  return HPC_OK;
+}
+
+int hpc_checkpoint_restore(hpc_ctx* c, const double* u, const double* v, const double* w, const double* H,
+                           const double* d, const double* d_old, const double* state6) {
+  if (!c || !u || !v || !w || !H || !d || !d_old || !state6) return arg_fail("null argument");
+  HPC_CUDA(cudaSetDevice(c->device));
+  const LevelGeo& g = c->L[c->maxlevel];
+  const double* src[6] = {u, v, w, H, d, d_old};
+  for (int i = 0; i < 6; ++i)
+    HPC_CUDA(cudaMemcpy2DAsync(ck_source(c, i), sizeof(double) * g.px, src[i], sizeof(double) * g.nx,
+                               sizeof(double) * g.nx, (size_t)g.ny * g.nz, cudaMemcpyHostToDevice, c->stream));
+  HPC_CUDA(cudaStreamSynchronize(c->stream));
+  return hpc_set_state(c, state6);
 }
 
 // ---------------------------------------------------------------- operators

@@ -93,6 +93,16 @@ struct hpc_ctx {
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
   int tev_cap, tev_used;
   double f_norm, fd_norm, Ue, Ut, dU, uprop;  // staggered-loop state (crack_propagation.cpp:32-39)
+  // checkpoint (hpc_checkpoint_*): a dense device snapshot of the finest u, v, w, H, d, d_old, copied
+  // to pinned host memory on a copy stream while the compute stream goes on
+  struct Checkpoint {
+    double* dev;   // 6 * nx*ny*nz doubles
+    double* host;  // pinned, same size
+    cudaStream_t stream;
+    cudaEvent_t snap, done;
+    int t, pending, valid;
+    double state[6];
+  } ck;
 };
 
 namespace hpc {

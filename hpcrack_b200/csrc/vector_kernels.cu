@@ -23,17 +23,25 @@ int num_sms_v() {
   return n;
 }
 
-// Row-structured launch: block rows (j,k) with a stride loop, threads over x.
+// Node-parallel launch: a grid-stride loop over the nx*ny*nz nodes of a level (flat, x fastest,
+// so neighbouring threads touch neighbouring addresses), at most 8 blocks of 256 threads per SM.
 constexpr int kRowThreads = 256;
 int row_grid(const LevelGeo& g, int per_sm = 8) {
-  long long rows = (long long)g.ny * g.nz;
-  long long cap = (long long)num_sms_v() * per_sm;
-  return (int)(rows < cap ? rows : cap);
+  const long long nodes = (long long)g.nx * g.ny * g.nz;
+  const long long blocks = (nodes + kRowThreads - 1) / kRowThreads;
+  const long long cap = (long long)num_sms_v() * per_sm;
+  return (int)(blocks < cap ? blocks : cap);
 }
 
-#define FOR_NODES(g)                                                                  \
-  for (long long row = blockIdx.x; row < (long long)(g).ny * (g).nz; row += gridDim.x) \
-    for (int i = threadIdx.x, j = (int)(row % (g).ny), kz = (int)(row / (g).ny); i < (g).nx; i += blockDim.x)
+// Level sizes stay below 2^31 nodes (hpc_create checks), so 32-bit index arithmetic suffices.  The
+// inner one-pass loop declares the node coordinates (i, j, kz) for the body; `continue` in the body
+// moves on to the next node.
+#define FOR_NODES(g)                                                                                 \
+  for (unsigned _f = blockIdx.x * blockDim.x + threadIdx.x, _nodes = (unsigned)((g).nx * (g).ny * (g).nz); \
+       _f < _nodes; _f += gridDim.x * blockDim.x)                                                     \
+    for (int i = (int)(_f % (unsigned)(g).nx), j = (int)((_f / (unsigned)(g).nx) % (unsigned)(g).ny),    \
+             kz = (int)(_f / ((unsigned)(g).nx * (unsigned)(g).ny)), _once = 1;                        \
+         _once; _once = 0)
 
 }  // namespace
 

@@ -68,6 +68,9 @@ SIGNATURES = {
     "hpc_download_choice": [_ctx, _i, C.POINTER(C.c_int16)],
     "hpc_get_state": [_ctx, _dp],
     "hpc_set_state": [_ctx, _dp],
+    "hpc_checkpoint_begin": [_ctx, _i],
+    "hpc_checkpoint_wait": [_ctx, _ip, C.POINTER(_dp), _dp],
+    "hpc_checkpoint_restore": [_ctx, _dp, _dp, _dp, _dp, _dp, _dp, _dp],
     "hpc_internal_force": [_ctx, _i, _i, _i, _d],
     "hpc_prem_u": [_ctx, _i, _i, _d],
     "hpc_fld": [_ctx, _i, _i, _i, _d],

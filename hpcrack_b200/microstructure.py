@@ -155,6 +155,35 @@ class Workload:
         return material_table()
 
 
+def hierarchy_for(nodes) -> tuple:
+    """(maxlevel, element_nb) for a box of `nodes` per axis: the deepest hierarchy whose coarsest
+    level keeps at least 8 elements on the shortest axis (a 9-node coarsest grid, as the
+    reference's configurations use) with every axis divisible by 2^maxlevel."""
+    elems = [int(n) - 1 for n in nodes]
+    L = 0
+    while all(e % (1 << (L + 1)) == 0 for e in elems) and min(elems) >> (L + 1) >= 8:
+        L += 1
+    return L, tuple(e >> L for e in elems)
+
+
+def inclusion_workload(name: str, nodes, seed: int, volume_fraction: float, maxlevel: int | None,
+                       increments: int) -> Workload:
+    """A two-phase inclusion specimen of the batched / served mixes: spheres with radii in [4, 8]
+    voxels scaled by the shortest axis / 64, to `volume_fraction`; materials, length scale and
+    load schedule of the 65^3 configuration; tolerance |r|/|f| <= 1e-8 (squared 1e-16)."""
+    nx, ny, nz = (int(n) for n in nodes)
+    s = (min(nx, ny, nz) - 1) / 64.0
+    img = sphere_image((nx, ny, nz), seed, [Phase(INCLUSION_GRAY, max(4 * s, 1.5), max(8 * s, 2.0),
+                                                  volume_fraction=volume_fraction)])
+    if maxlevel is None:
+        maxlevel, enb = hierarchy_for((nx, ny, nz))
+    else:
+        enb = tuple((n - 1) >> maxlevel for n in (nx, ny, nz))
+    return Workload(name, img, enb, maxlevel, (0.0, 0.0, 0.0), 1e-6, 2.0, 1e-6, (50, 4, 2, 1, 200),
+                    (10, 2, 1, 1, 200), increments, ut0=1e-4 * (nz - 1), du=1e-4 * (nz - 1), mech_tol=1e-16,
+                    pf_tol=1e-16)
+
+
 def make_workload(name: str) -> Workload:
     """Seeded synthetic stand-ins for the benchmark configurations.
 
@@ -162,6 +191,8 @@ def make_workload(name: str) -> Workload:
       3 increments of 1e-4*Nz top displacement; tolerance |r|/|f| <= 1e-8.
     * ``plain257``  257^3, seed 1, inclusions r in [6,20] to 25 %, pores r in [3,8] to 5 %;
       pre-crack at mid-height over half the x width; 20 increments.
+    * ``mid129`` / ``mid193``  the plain257 recipe scaled to 129^3 / 193^3 (193: element_nb 12), for
+      profiling at a few GB of device memory.
     * ``large513``  513^3, seed 2, inclusions to 30 %.
     * ``small17`` / ``small33`` test-sized variants of parity65.
     """
@@ -172,12 +203,13 @@ def make_workload(name: str) -> Workload:
         return Workload(name, img, (8, 8, 8), maxlevel_for(n, 0, 8), (0.0, 0.0, 0.0), 1e-6, 2.0, 1e-6,
                         (50, 4, 2, 1, 200), (10, 2, 1, 1, 200), 3, ut0=1e-4 * (n - 1), du=1e-4 * (n - 1),
                         mech_tol=1e-16, pf_tol=1e-16)
-    if name in ("plain257", "mid129"):
-        n = 257 if name == "plain257" else 129
+    if name in ("plain257", "mid129", "mid193"):
+        n = {"plain257": 257, "mid129": 129, "mid193": 193}[name]
+        enb = 12 if n == 193 else 8  # 193 = 12 * 2^4 + 1
         s = (n - 1) / 256.0
         img = sphere_image((n, n, n), 1, [Phase(INCLUSION_GRAY, 6 * s, 20 * s, volume_fraction=0.25),
                                           Phase(PORE_GRAY, max(3 * s, 1.5), 8 * s, volume_fraction=0.05)])
-        return Workload(name, img, (8, 8, 8), maxlevel_for(n, 0, 8), (0.0, 0.0, 0.0), 1e-6, 2.0, 1e-6,
+        return Workload(name, img, (enb, enb, enb), maxlevel_for(n, 0, enb), (0.0, 0.0, 0.0), 1e-6, 2.0, 1e-6,
                         (50, 4, 2, 1, 200), (10, 2, 1, 1, 200), 20, ut0=1e-4 * (n - 1), du=1e-4 * (n - 1),
                         mech_tol=1e-16, pf_tol=1e-16, crack={"H": 1e6, "layer": (n - 1) // 2, "xfrac": 0.5})
     if name == "large513":

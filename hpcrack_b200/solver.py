@@ -131,6 +131,28 @@ class Hierarchy:
     def set_state(self, s6):
         self._c("hpc_set_state", (C.c_double * 6)(*s6))
 
+    # ------------------------------------------------------------ checkpoint / restart
+    CHECKPOINT_FIELDS = ("u", "v", "w", "H", "d", "d_old")
+
+    def checkpoint_begin(self, t: int):
+        """Snapshot the loop state on the device and start its copy to host memory (asynchronous)."""
+        self._c("hpc_checkpoint_begin", int(t))
+
+    def checkpoint_wait(self):
+        """-> (t, {name: dense finest array}, state6) of the last checkpoint_begin (copies made)."""
+        t = C.c_int(0)
+        p = C.POINTER(C.c_double)()
+        s = (C.c_double * 6)()
+        self._c("hpc_checkpoint_wait", C.byref(t), C.byref(p), s)
+        nn = self.n(self.maxlevel)
+        flat = np.ctypeslib.as_array(p, shape=(6 * nn,)).copy()
+        return t.value, {k: flat[i * nn:(i + 1) * nn] for i, k in enumerate(self.CHECKPOINT_FIELDS)}, list(s)
+
+    def checkpoint_restore(self, fields: dict, state6):
+        arrs = [np.ascontiguousarray(fields[k], dtype=np.float64).reshape(self.n(self.maxlevel))
+                for k in self.CHECKPOINT_FIELDS]
+        self._c("hpc_checkpoint_restore", *[_dptr(a) for a in arrs], (C.c_double * 6)(*state6))
+
     def launch_count(self, reset=False) -> int:
         v = C.c_longlong(0)
         self._c("hpc_launch_count", C.byref(v), int(reset))

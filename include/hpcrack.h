@@ -134,6 +134,23 @@ int hpc_download_choice(hpc_ctx* ctx, int level, int16_t* host);
 int hpc_get_state(hpc_ctx* ctx, double* s6);
 int hpc_set_state(hpc_ctx* ctx, const double* s6);
 
+/* ---------------- checkpoint / restart ---------------- */
+/* The history dumps of crack_propagation.cpp:99-106 (write_vector_3D of u, v, w, H, d,
+ * write_read_history.cpp:18-53) made restartable: the finest u (3 components), H, d and d_old plus
+ * the loop state are snapshotted on the device (dense x-fastest, the reference's file order) and
+ * copied to pinned host memory on a separate stream, overlapping the increments that follow.  The
+ * first call allocates 6 dense finest-level arrays on the device and in pinned host memory. */
+int hpc_checkpoint_begin(hpc_ctx* ctx, int t);
+/* Waits for the copy of the last hpc_checkpoint_begin.  *fields points to 6 consecutive dense
+ * arrays of nx*ny*nz doubles (u, v, w, H, d, d_old), valid until the next hpc_checkpoint_begin or
+ * hpc_destroy; state6 as hpc_get_state at the time of the snapshot; *t the index given to begin.
+ * Each output may be null. */
+int hpc_checkpoint_wait(hpc_ctx* ctx, int* t, const double** fields, double* state6);
+/* Restores a checkpoint into the finest level (read_vector_3D, write_read_history.cpp:55-86, for
+ * the fields) and the loop state; the next hpc_step continues as the uninterrupted run would. */
+int hpc_checkpoint_restore(hpc_ctx* ctx, const double* u, const double* v, const double* w, const double* H,
+                           const double* d, const double* d_old, const double* state6);
+
 /* ---------------- operators ---------------- */
 /* Internal_Force: dst = K(d) src on one level (mechanical_pcg.cpp:174-191). */
 int hpc_internal_force(hpc_ctx* ctx, int level, int src_field, int dst_field, double small_k);

@@ -389,6 +389,8 @@ class RefOracle(_Base):
             "step": (C.c_int, [vp, C.c_int, _ip, _ip, C.c_double, C.c_double, C.c_double, C.c_double,
                                C.c_double, C.c_double, _dp]),
             "last_output": (C.c_char_p, []),
+            "write_vector_3d": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]),
+            "read_vector_3d": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]),
         }
 
     def _create(self, maxlevel, enb, x0, roi):
@@ -445,3 +447,13 @@ class RefOracle(_Base):
 
     def last_output(self) -> str:
         return self.lib.ref_last_output().decode(errors="replace")
+
+    def write_vector_3d(self, field, level, comp, path, t=0):
+        """The reference's write_vector_3D (write_read_history.cpp:18-53) of one grid to `path`."""
+        if self.lib.ref_write_vector_3d(self.h, field, level, comp, path.encode(), t) != 0:
+            raise ValueError("bad field")
+
+    def read_vector_3d(self, field, level, comp, path, t=0):
+        """The reference's read_vector_3D (write_read_history.cpp:55-86) of `path` into one grid."""
+        if self.lib.ref_read_vector_3d(self.h, field, level, comp, path.encode(), t) != 0:
+            raise ValueError("bad field")

@@ -44,6 +44,7 @@
 #include "boundary_conditions.h"
 #include "image_input.h"
 #include "pcg_utilities.h"
+#include "write_read_history.h"
 
 namespace {
 
@@ -606,5 +607,20 @@ void ref_set_state(void* h, const double* s6) {
 
 /* Text the reference printed during the last captured call (residual history). */
 const char* ref_last_output(void) { return g_last_out.c_str(); }
+
+// write_vector_3D / read_vector_3D (write_read_history.cpp:18-86) of one grid; `path` ends in
+// ".dat", so the reference uses it as given.
+int ref_write_vector_3d(void* h, int field, int level, int comp, const char* path, int t) {
+  griddouble* g = grid_of((RefCtx*)h, field, level, comp);
+  if (!g) return -1;
+  captured([&] { write_vector_3D(*g, std::string(path), 0, t); });
+  return 0;
+}
+int ref_read_vector_3d(void* h, int field, int level, int comp, const char* path, int t) {
+  griddouble* g = grid_of((RefCtx*)h, field, level, comp);
+  if (!g) return -1;
+  captured([&] { read_vector_3D(*g, std::string(path), 0, t); });
+  return 0;
+}
 
 }  // extern "C"
