@@ -34,9 +34,12 @@ METRIC = "MDoF-iter/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 PCG_APPLY_BYTES_PER_NODE = 73
-# DRAM bytes (read + write) per launch of the finest PCG apply, from one ncu capture per workload
-# (None until captured); a 257^3 figure is the 193^3 capture scaled by the node count.
-PCG_APPLY_TRAFFIC = {}
+MECH_SOLVERS = {"fas": 0, "fcg": 1, "mixed": 2}
+# DRAM bytes (read + write) per launch of the finest PCG apply: the ncu capture of
+# profiles/mech_pcg_apply_mid193.md measured 440.5 MB + 153.1 MB on the 193^3 level (7,189,057 nodes,
+# 82.6 B/node); other sizes scale that per-node figure by their node count (traffic grows with the
+# nodes, the strip-edge re-reads included).
+PCG_APPLY_TRAFFIC_PER_NODE = (440.516864e6 + 153.093120e6) / 193 ** 3
 
 
 def parse_args():
@@ -46,6 +49,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--workload", default="plain257")
+    ap.add_argument("--mech-solver", choices=("fas", "fcg", "mixed"), default="fas",
+                    help="fas: the reference's FAS V-cycles (plain form); fcg: flexible PCG preconditioned by one "
+                         "FP64 V-cycle per iteration; mixed: the precision form (FP32 V-cycle, FP64 outer PCG)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-timing", action="store_true")
@@ -60,6 +66,9 @@ def parse_args():
                          "admission server; prints solves/s and p50/p99 latency")
     ap.add_argument("--batch", type=int, default=0, metavar="N",
                     help="batched form: N specimens of the uneven-size mix (seeds 100..) submitted at once")
+    ap.add_argument("--compare-forms", action="store_true",
+                    help="run --steps increments with the plain form and with --mech-solver (default mixed) and "
+                         "report solves/s of both and the per-field error against the plain run")
     ap.add_argument("--requests", type=int, default=24, help="requests in a --serve sample")
     ap.add_argument("--increments", type=int, default=0, help="increments per request (default 10 serve, 5 batch)")
     ap.add_argument("--slots", type=int, default=8, help="concurrent requests on the GPU")
@@ -88,7 +97,8 @@ def run_serving(args, local):
         reqs = sv.serve_mix(args.requests, args.serve, seed=7, increments=inc, **kw)
         metric, form = "solves/s", f"served: {args.requests} requests, Poisson arrivals at {args.serve}/s (seed 7), " \
                                    f"{inc} increments each"
-    srv = sv.SolveServer(budget, args.slots, solver_factory=sv.default_factory(local))
+    srv = sv.SolveServer(budget, args.slots, solver_factory=sv.default_factory(local),
+                         mech_solver=MECH_SOLVERS[args.mech_solver])
     t0 = time.perf_counter()
     res = srv.replay(reqs)
     wall = time.perf_counter() - t0
@@ -99,7 +109,8 @@ def run_serving(args, local):
         dof_iters += sum(3.0 * nx * ny * nz * o[6] + nx * ny * nz * o[7] for o in r.outputs)
     line = {"metric": metric, "value": st["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
             "dtype": "f64", "data": "synthetic", "config": {"workload": form, "slots": args.slots,
-                                                            "hbm_budget_gb": args.hbm_budget_gb},
+                                                            "hbm_budget_gb": args.hbm_budget_gb,
+                                                            "mech_solver": args.mech_solver},
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "wall_s": wall,
             "mdof_iter_per_s": dof_iters / wall / 1e6, "peak_active": srv.peak_active,
             "peak_hbm_gb": srv.peak_used / (1 << 30)}
@@ -129,7 +140,8 @@ def run_profile_cycles(args, local):
     mg_d = tuple(w.mg_d[:4]) + (K,)
     launches0 = hier.launch_count()
     outs = [hier.step(t, mg_u, mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du, dU_factor=w.du_factor,
-                      mech_tol=w.mech_tol, pf_tol=w.pf_tol) for t in range(2)]
+                      mech_tol=w.mech_tol, pf_tol=w.pf_tol, mech_solver=MECH_SOLVERS[args.mech_solver])
+            for t in range(2)]
     hier.sync()
     print(json.dumps({"profile_cycles": K, "workload": w.name, "launches": hier.launch_count() - launches0,
                       "mech_cycles": [int(o[4]) for o in outs], "pf_cycles": [int(o[5]) for o in outs]}), flush=True)
@@ -283,14 +295,18 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------------------------
-def workload_config(w, world):
+def workload_config(w, world, mech_solver="fas"):
     nx, ny, nz = w.nodes
     return {"workload": f"{w.name}: {nx}x{ny}x{nz}-node three-phase inclusion/pore specimen, pre-cracked, "
                         f"staggered increments (mechanical + phase-field FAS V-cycles, plain FP64)",
             "nodes": nx * ny * nz, "mech_dof": 3 * nx * ny * nz, "levels": w.maxlevel + 1,
             "element_nb": list(w.element_nb), "mg_u": list(w.mg_u), "mg_d": list(w.mg_d),
             "mech_tol_sq": w.mech_tol, "pf_tol_sq": w.pf_tol, "replicas": world, "parallelism": f"replicas{world}",
-            "l2": "inputs larger than L2 (each finest field 136 MB > 126 MB), no flush"}
+            "l2": "inputs larger than L2 (each finest field 136 MB > 126 MB), no flush",
+            "mech_solver": {"fas": "FAS V-cycles with restarted Jacobi-PCG smoothers (the reference's method)",
+                            "fcg": "flexible PCG (FP64) preconditioned by one V-cycle per iteration",
+                            "mixed": "precision form: flexible PCG (FP64 residual, dots, updates) preconditioned by "
+                                     "one FP32 V-cycle (FP64 coarsest solve)"}[mech_solver]}
 
 
 def load_specimen(w, device):
@@ -328,9 +344,11 @@ def run_b200(args, rank, world, local):
     hier = load_specimen(w, local)
     stream = torch.cuda.ExternalStream(hier.stream())
 
+    solver = MECH_SOLVERS[args.mech_solver]
+
     def step(t):
         return hier.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
-                         dU_factor=w.du_factor, mech_tol=w.mech_tol, pf_tol=w.pf_tol)
+                         dU_factor=w.du_factor, mech_tol=w.mech_tol, pf_tol=w.pf_tol, mech_solver=solver)
 
     t = 0
     for _ in range(args.warmup):
@@ -377,8 +395,9 @@ def run_b200(args, rank, world, local):
         peak, src = peaks()
         roofline = {"bound": "hbm", "kernel": "mech_kernel<finest, PCG> (w = K(d) p, (p, w))",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "peak_source": src, "traffic": PCG_APPLY_TRAFFIC.get(w.name), "launches": kn,
-                    "avg_launch_ms": kms / kn, "bytes_per_node": PCG_APPLY_BYTES_PER_NODE}
+                    "peak_source": src, "traffic": PCG_APPLY_TRAFFIC_PER_NODE * N,
+                    "traffic_note": "bytes per launch: ncu dram bytes per node of the 193^3 capture x nodes",
+                    "launches": kn, "avg_launch_ms": kms / kn, "bytes_per_node": PCG_APPLY_BYTES_PER_NODE}
 
     # ------------------------------------------------------------ end to end through the C ABI
     e2e = None
@@ -434,13 +453,56 @@ def run_b200(args, rank, world, local):
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": workload_config(w, world), "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+                "config": workload_config(w, world, args.mech_solver), "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
                 "roofline": roofline, "cpu_baseline": cpu,
                 "solves_per_s": world * args.steps / (max_ms / 1e3),
                 "steps_detail": [{"t": t_first + i, "mech_cycles": int(o[4]), "pf_cycles": int(o[5]),
                                   "mech_iters": int(o[6]), "pf_iters": int(o[7]), "F": o[1], "dmax": o[3]}
                                  for i, o in enumerate(outs)]}
         print(json.dumps(line), flush=True)
+
+
+def run_compare_forms(args, local):
+    """Precision form against the plain FP64 form on the same specimen: both run the same increments
+    to the same FP64 stopping test; prints solves/s of each and the per-field L2 / max error of the
+    precision form's u, d, H relative to the plain run."""
+    import numpy as np
+    import torch
+    from hpcrack_b200 import microstructure as ms
+    from hpcrack_b200.solver import U, D, H
+    torch.cuda.set_device(local)
+    w = ms.make_workload(args.workload)
+    res = {}
+    for name in ("fas", args.mech_solver if args.mech_solver != "fas" else "mixed"):
+        hier = load_specimen(w, local)
+        stream = torch.cuda.ExternalStream(hier.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        outs = [hier.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
+                          dU_factor=w.du_factor, mech_tol=w.mech_tol, pf_tol=w.pf_tol,
+                          mech_solver=MECH_SOLVERS[name]) for t in range(args.steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_tot = e0.elapsed_time(e1)
+        res[name] = {"outs": outs, "ms": ms_tot, "fields": {k: hier.get(f, w.maxlevel) for k, f in
+                                                              (("u", U), ("d", D), ("H", H))}}
+        hier.close()
+    plain, other = res["fas"], res[[k for k in res if k != "fas"][0]]
+    errs = {}
+    for k in ("u", "d", "H"):
+        a, b = other["fields"][k], plain["fields"][k]
+        nb = float(np.linalg.norm(b))
+        errs[k] = {"rel_l2": float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0),
+                   "max_abs": float(np.max(np.abs(a - b))), "max_ref": float(np.max(np.abs(b)))}
+    line = {"metric": "solves/s", "workload": w.name, "increments": args.steps,
+            "plain": {"solves_per_s": args.steps / (plain["ms"] / 1e3), "ms": plain["ms"],
+                      "v_cycles": [int(o[4]) for o in plain["outs"]]},
+            "form": {"name": [k for k in res if k != "fas"][0], "solves_per_s": args.steps / (other["ms"] / 1e3),
+                     "ms": other["ms"], "v_cycles": [int(o[4]) for o in other["outs"]]},
+            "speedup": plain["ms"] / other["ms"], "field_error_vs_plain": errs,
+            "reaction_rel_diff": [abs(a[1] - b[1]) / abs(b[1]) for a, b in zip(other["outs"], plain["outs"])]}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -453,6 +515,8 @@ def main():
             run_profile_cycles(args, local)
         elif args.serve or args.batch:
             run_serving(args, local)
+        elif args.compare_forms:
+            run_compare_forms(args, local)
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

@@ -120,17 +120,26 @@ __device__ __forceinline__ BcFlags bc_flags(const LevelGeo& g, int i, int j, int
 // 1 - t and t, the 1-D derivative is (u1 - u0)/h, as in Dshape_function (shape_function.cpp:16-75).
 // Every Gauss point carries the same weight wg = hx*hy*hz/8, which callers fold into the material.
 // ---------------------------------------------------------------------------------------------
-struct SF {
-  double t[2];
-  double ih[3];  // 1/hx, 1/hy, 1/hz
+template <typename T>
+struct SFt {
+  T t[2];
+  T ih[3];  // 1/hx, 1/hy, 1/hz
 };
+using SF = SFt<double>;
+
+// x == +-0 from the bit pattern (integer pipe); v exactly zero is what gauss_point_MP tests.
+__device__ __forceinline__ bool bits_zero(double v) { return (__double_as_longlong(v) << 1) == 0; }
+__device__ __forceinline__ bool bits_zero(float v) { return (__float_as_uint(v) << 1) == 0u; }
 
 // Gradient of a trilinear field at the 8 Gauss points.  d/dx is independent of the x Gauss index,
 // so it has 4 distinct values gx[p + 2r]; likewise gy[q + 2r], gz[q + 2p].  Optionally the values
-// at the Gauss points, val[q + 2p + 4r].
-__device__ __forceinline__ void sf_forward(const double (&u)[8], const SF& s, double (&gx)[4],
-                                           double (&gy)[4], double (&gz)[4], double* val) {
-  double dx[4], ix[2][4], dy[2][2];
+// at the Gauss points, val[q + 2p + 4r].  ISO (hx = hy = hz): the gradients are left unscaled by
+// 1/h; callers fold 1/h^2 into the material, which is exact when h is a power of two (every level
+// of a hierarchy whose finest spacing is 1, as the reference's voxel domains have).
+template <bool ISO = false, typename T>
+__device__ __forceinline__ void sf_forward(const T (&u)[8], const SFt<T>& s, T (&gx)[4], T (&gy)[4], T (&gz)[4],
+                                           T* val) {
+  T dx[4], ix[2][4], dy[2][2];
 #pragma unroll
   for (int bc = 0; bc < 4; ++bc) dx[bc] = u[2 * bc + 1] - u[2 * bc];
 #pragma unroll
@@ -145,10 +154,10 @@ __device__ __forceinline__ void sf_forward(const double (&u)[8], const SF& s, do
   for (int q = 0; q < 2; ++q)
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
-      const double i0 = fma(s.t[p], dy[q][0], ix[q][0]);
-      const double i1 = fma(s.t[p], dy[q][1], ix[q][2]);
-      const double dz = i1 - i0;
-      gz[q + 2 * p] = dz * s.ih[2];
+      const T i0 = fma(s.t[p], dy[q][0], ix[q][0]);
+      const T i1 = fma(s.t[p], dy[q][1], ix[q][2]);
+      const T dz = i1 - i0;
+      gz[q + 2 * p] = ISO ? dz : dz * s.ih[2];
       if (val) {
         val[q + 2 * p] = fma(s.t[0], dz, i0);
         val[q + 2 * p + 4] = fma(s.t[1], dz, i0);
@@ -156,56 +165,64 @@ __device__ __forceinline__ void sf_forward(const double (&u)[8], const SF& s, do
     }
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
-    const double e = dy[q][1] - dy[q][0];
+    const T e = dy[q][1] - dy[q][0];
 #pragma unroll
-    for (int r = 0; r < 2; ++r) gy[q + 2 * r] = fma(s.t[r], e, dy[q][0]) * s.ih[1];
+    for (int r = 0; r < 2; ++r) {
+      const T v = fma(s.t[r], e, dy[q][0]);
+      gy[q + 2 * r] = ISO ? v : v * s.ih[1];
+    }
   }
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
-    const double e0 = fma(s.t[p], dx[1] - dx[0], dx[0]);
-    const double e1 = fma(s.t[p], dx[3] - dx[2], dx[2]);
-    const double e = e1 - e0;
+    const T e0 = fma(s.t[p], dx[1] - dx[0], dx[0]);
+    const T e1 = fma(s.t[p], dx[3] - dx[2], dx[2]);
+    const T e = e1 - e0;
 #pragma unroll
-    for (int r = 0; r < 2; ++r) gx[p + 2 * r] = fma(s.t[r], e, e0) * s.ih[0];
+    for (int r = 0; r < 2; ++r) {
+      const T v = fma(s.t[r], e, e0);
+      gx[p + 2 * r] = ISO ? v : v * s.ih[0];
+    }
   }
 }
 
 // Exact transpose of sf_forward: given adjoints of gx, gy, gz (and optionally of the Gauss-point
 // values), accumulates the nodal adjoint f[8] (f is overwritten).
-__device__ __forceinline__ void sf_adjoint(const double (&sgx)[4], const double (&sgy)[4],
-                                           const double (&sgz)[4], const double* sval, const SF& s,
-                                           double (&f)[8]) {
-  const double t0 = s.t[0], t1 = s.t[1], u0 = 1.0 - t0, u1 = 1.0 - t1;
+template <bool ISO = false, typename T>
+__device__ __forceinline__ void sf_adjoint(const T (&sgx)[4], const T (&sgy)[4], const T (&sgz)[4], const T* sval,
+                                           const SFt<T>& s, T (&f)[8]) {
+  const T t0 = s.t[0], t1 = s.t[1], u0 = T(1) - t0, u1 = T(1) - t1;
   // gx[p+2r] = ih0 * ((1-t_r) ey[p][0] + t_r ey[p][1]);  ey[p][c] = (1-t_p) dx[2c] + t_p dx[2c+1]
-  double Adx[4];
+  T Adx[4];
   {
-    double a00 = sgx[0] * s.ih[0], a10 = sgx[1] * s.ih[0], a01 = sgx[2] * s.ih[0], a11 = sgx[3] * s.ih[0];
+    const T ihx = s.ih[0];
+    const T a00 = ISO ? sgx[0] : sgx[0] * ihx, a10 = ISO ? sgx[1] : sgx[1] * ihx;
+    const T a01 = ISO ? sgx[2] : sgx[2] * ihx, a11 = ISO ? sgx[3] : sgx[3] * ihx;
     // Aey[p][c]
-    const double e00 = u0 * a00 + u1 * a01, e01 = t0 * a00 + t1 * a01;  // p = 0
-    const double e10 = u0 * a10 + u1 * a11, e11 = t0 * a10 + t1 * a11;  // p = 1
+    const T e00 = u0 * a00 + u1 * a01, e01 = t0 * a00 + t1 * a01;  // p = 0
+    const T e10 = u0 * a10 + u1 * a11, e11 = t0 * a10 + t1 * a11;  // p = 1
     Adx[0] = u0 * e00 + u1 * e10;
     Adx[1] = t0 * e00 + t1 * e10;
     Adx[2] = u0 * e01 + u1 * e11;
     Adx[3] = t0 * e01 + t1 * e11;
   }
   // gy[q+2r] = ih1 * ((1-t_r) dy[q][0] + t_r dy[q][1])
-  double Ady[2][2];
+  T Ady[2][2];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
-    const double a0 = sgy[q] * s.ih[1], a1 = sgy[q + 2] * s.ih[1];
+    const T a0 = ISO ? sgy[q] : sgy[q] * s.ih[1], a1 = ISO ? sgy[q + 2] : sgy[q + 2] * s.ih[1];
     Ady[q][0] = u0 * a0 + u1 * a1;
     Ady[q][1] = t0 * a0 + t1 * a1;
   }
   // gz[q+2p] = ih2 * (iy[q][p][1] - iy[q][p][0]);  val = iy[q][p][0] + t_r (iy[..][1] - iy[..][0])
-  double Aiy[2][2][2];
+  T Aiy[2][2][2];
 #pragma unroll
   for (int q = 0; q < 2; ++q)
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
-      double adz = sgz[q + 2 * p] * s.ih[2];
-      double a0 = 0.0;
+      T adz = ISO ? sgz[q + 2 * p] : sgz[q + 2 * p] * s.ih[2];
+      T a0 = T(0);
       if (sval) {
-        const double v0 = sval[q + 2 * p], v1 = sval[q + 2 * p + 4];
+        const T v0 = sval[q + 2 * p], v1 = sval[q + 2 * p + 4];
         adz += t0 * v0 + t1 * v1;
         a0 = v0 + v1;
       }
@@ -213,31 +230,32 @@ __device__ __forceinline__ void sf_adjoint(const double (&sgx)[4], const double 
       Aiy[q][p][0] = a0 - adz;
     }
   // iy[q][p][c] = ix[q][2c] + t_p dy[q][c];  dy[q][c] = ix[q][2c+1] - ix[q][2c]
-  double Aix[2][4];
+  T Aix[2][4];
 #pragma unroll
   for (int q = 0; q < 2; ++q)
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-      const double s0 = Aiy[q][0][c] + Aiy[q][1][c];
-      const double ady = Ady[q][c] + t0 * Aiy[q][0][c] + t1 * Aiy[q][1][c];
+      const T s0 = Aiy[q][0][c] + Aiy[q][1][c];
+      const T ady = Ady[q][c] + t0 * Aiy[q][0][c] + t1 * Aiy[q][1][c];
       Aix[q][2 * c + 1] = ady;
       Aix[q][2 * c] = s0 - ady;
     }
   // ix[q][bc] = u[2bc] + t_q dx[bc];  dx[bc] = u[2bc+1] - u[2bc]
 #pragma unroll
   for (int bc = 0; bc < 4; ++bc) {
-    const double adx = Adx[bc] + t0 * Aix[0][bc] + t1 * Aix[1][bc];
+    const T adx = Adx[bc] + t0 * Aix[0][bc] + t1 * Aix[1][bc];
     f[2 * bc + 1] = adx;
     f[2 * bc] = Aix[0][bc] + Aix[1][bc] - adx;
   }
 }
 
 // Trilinear values of a nodal field at the 8 Gauss points.
-__device__ __forceinline__ void sf_interp(const double (&v)[8], const SF& s, double (&out)[8]) {
-  double ix[2][4];
+template <typename T>
+__device__ __forceinline__ void sf_interp(const T (&v)[8], const SFt<T>& s, T (&out)[8]) {
+  T ix[2][4];
 #pragma unroll
   for (int bc = 0; bc < 4; ++bc) {
-    const double d = v[2 * bc + 1] - v[2 * bc];
+    const T d = v[2 * bc + 1] - v[2 * bc];
     ix[0][bc] = fma(s.t[0], d, v[2 * bc]);
     ix[1][bc] = fma(s.t[1], d, v[2 * bc]);
   }
@@ -245,9 +263,9 @@ __device__ __forceinline__ void sf_interp(const double (&v)[8], const SF& s, dou
   for (int q = 0; q < 2; ++q)
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
-      const double i0 = fma(s.t[p], ix[q][1] - ix[q][0], ix[q][0]);
-      const double i1 = fma(s.t[p], ix[q][3] - ix[q][2], ix[q][2]);
-      const double dz = i1 - i0;
+      const T i0 = fma(s.t[p], ix[q][1] - ix[q][0], ix[q][0]);
+      const T i1 = fma(s.t[p], ix[q][3] - ix[q][2], ix[q][2]);
+      const T dz = i1 - i0;
       out[q + 2 * p] = fma(s.t[0], dz, i0);
       out[q + 2 * p + 4] = fma(s.t[1], dz, i0);
     }
@@ -255,13 +273,14 @@ __device__ __forceinline__ void sf_interp(const double (&v)[8], const SF& s, dou
 
 // gauss_point_MP (material_gauss_point.cpp:18-41): 0 at every Gauss point if any nodal value is
 // exactly 0, else the trilinear values.
-__device__ __forceinline__ void gp_material(const double (&v)[8], const SF& s, double (&out)[8]) {
-  bool zero = false;
+template <typename T>
+__device__ __forceinline__ void gp_material(const T (&v)[8], const SFt<T>& s, T (&out)[8]) {
+  bool zero = false;  // v == +-0, tested on the bit pattern (integer pipe, not the floating-point unit)
 #pragma unroll
-  for (int n = 0; n < 8; ++n) zero |= (v[n] == 0.0);
+  for (int n = 0; n < 8; ++n) zero |= bits_zero(v[n]);
   if (zero) {
 #pragma unroll
-    for (int g = 0; g < 8; ++g) out[g] = 0.0;
+    for (int g = 0; g < 8; ++g) out[g] = T(0);
   } else {
     sf_interp(v, s, out);
   }
@@ -270,16 +289,17 @@ __device__ __forceinline__ void gp_material(const double (&v)[8], const SF& s, d
 // Element stiffness action K_e u_e for Q1 small-strain elasticity with per-Gauss-point moduli
 // (Internal_Force_element, mechanical_pcg.cpp:114-172): sigma = K tr(eps) I + 2G dev(eps).
 // Kw, Gw already include the Gauss weight wg.
-__device__ __forceinline__ void mech_element(const double (&u)[3][8], const double (&Kw)[8],
-                                             const double (&Gw)[8], const SF& s, double (&f)[3][8]) {
-  double gx[3][4], gy[3][4], gz[3][4];
+template <bool ISO = false, typename T>
+__device__ __forceinline__ void mech_element(const T (&u)[3][8], const T (&Kw)[8], const T (&Gw)[8],
+                                             const SFt<T>& s, T (&f)[3][8]) {
+  T gx[3][4], gy[3][4], gz[3][4];
 #pragma unroll
-  for (int m = 0; m < 3; ++m) sf_forward(u[m], s, gx[m], gy[m], gz[m], nullptr);
-  double sx[3][4], sy[3][4], sz[3][4];
+  for (int m = 0; m < 3; ++m) sf_forward<ISO>(u[m], s, gx[m], gy[m], gz[m], (T*)nullptr);
+  T sx[3][4], sy[3][4], sz[3][4];
 #pragma unroll
   for (int m = 0; m < 3; ++m)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) sx[m][i] = sy[m][i] = sz[m][i] = 0.0;
+    for (int i = 0; i < 4; ++i) sx[m][i] = sy[m][i] = sz[m][i] = T(0);
 #pragma unroll
   for (int r = 0; r < 2; ++r)
 #pragma unroll
@@ -287,22 +307,22 @@ __device__ __forceinline__ void mech_element(const double (&u)[3][8], const doub
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const int g = q + 2 * p + 4 * r, ix = p + 2 * r, iy = q + 2 * r, iz = q + 2 * p;
-        const double exx = gx[0][ix], eyy = gy[1][iy], ezz = gz[2][iz];
-        const double gxy = gx[1][ix] + gy[0][iy];
-        const double gxz = gx[2][ix] + gz[0][iz];
-        const double gyz = gy[2][iy] + gz[1][iz];
-        const double K = Kw[g], G = Gw[g];
-        const double tr = exx + eyy + ezz;
-        const double lt = fma(-2.0 / 3.0, G, K) * tr;
-        const double G2 = G + G;
-        const double sxx = fma(G2, exx, lt), syy = fma(G2, eyy, lt), szz = fma(G2, ezz, lt);
-        const double sxy = G * gxy, sxz = G * gxz, syz = G * gyz;
+        const T exx = gx[0][ix], eyy = gy[1][iy], ezz = gz[2][iz];
+        const T gxy = gx[1][ix] + gy[0][iy];
+        const T gxz = gx[2][ix] + gz[0][iz];
+        const T gyz = gy[2][iy] + gz[1][iz];
+        const T K = Kw[g], G = Gw[g];
+        const T tr = exx + eyy + ezz;
+        const T lt = fma(T(-2.0 / 3.0), G, K) * tr;
+        const T G2 = G + G;
+        const T sxx = fma(G2, exx, lt), syy = fma(G2, eyy, lt), szz = fma(G2, ezz, lt);
+        const T sxy = G * gxy, sxz = G * gxz, syz = G * gyz;
         sx[0][ix] += sxx; sx[1][ix] += sxy; sx[2][ix] += sxz;
         sy[0][iy] += sxy; sy[1][iy] += syy; sy[2][iy] += syz;
         sz[0][iz] += sxz; sz[1][iz] += syz; sz[2][iz] += szz;
       }
 #pragma unroll
-  for (int m = 0; m < 3; ++m) sf_adjoint(sx[m], sy[m], sz[m], nullptr, s, f[m]);
+  for (int m = 0; m < 3; ++m) sf_adjoint<ISO>(sx[m], sy[m], sz[m], (const T*)nullptr, s, f[m]);
 }
 
 // Diagonal of the element stiffness (PreM_u_element, mechanical_pcg.cpp:63-100):
@@ -343,10 +363,11 @@ __device__ __forceinline__ void mech_element_diag(const double (&Kw)[8], const d
 
 // Phase-field element action (Fld_element, phase_field_pcg.cpp:61-91):
 //   f_sf = sum_g [aw_g N_sf x_g + bw_g dN_sf . dx_g],  aw = wg (2H + gc_g/lc), bw = wg gc_g lc.
+template <bool ISO = false>
 __device__ __forceinline__ void pf_element(const double (&x)[8], const double (&aw)[8], const double (&bw)[8],
                                            const SF& s, double (&f)[8]) {
   double gx[4], gy[4], gz[4], val[8];
-  sf_forward(x, s, gx, gy, gz, val);
+  sf_forward<ISO>(x, s, gx, gy, gz, val);
   double sgx[4] = {0, 0, 0, 0}, sgy[4] = {0, 0, 0, 0}, sgz[4] = {0, 0, 0, 0}, sv[8];
 #pragma unroll
   for (int r = 0; r < 2; ++r)
@@ -360,7 +381,7 @@ __device__ __forceinline__ void pf_element(const double (&x)[8], const double (&
         sgy[q + 2 * r] = fma(bw[g], gy[q + 2 * r], sgy[q + 2 * r]);
         sgz[q + 2 * p] = fma(bw[g], gz[q + 2 * p], sgz[q + 2 * p]);
       }
-  sf_adjoint(sgx, sgy, sgz, sv, s, f);
+  sf_adjoint<ISO>(sgx, sgy, sgz, sv, s, f);
 }
 
 // Diagonal of the phase-field element matrix (Md_element, phase_field_pcg.cpp:20-47).
@@ -417,14 +438,15 @@ __device__ __forceinline__ double phi_neg(double K, const Strain& e) {
   return tr >= 0 ? 0.0 : 0.5 * K * tr * tr;
 }
 
-__device__ __forceinline__ SF make_sf(const LevelGeo& g) {
-  SF s;
+template <typename T = double>
+__device__ __forceinline__ SFt<T> make_sf(const LevelGeo& g) {
+  SFt<T> s;
   const double r3 = 0.57735026918962584;  // 1/sqrt(3)
-  s.t[0] = 0.5 * (1.0 - r3);
-  s.t[1] = 0.5 * (1.0 + r3);
-  s.ih[0] = 1.0 / g.hx;
-  s.ih[1] = 1.0 / g.hy;
-  s.ih[2] = 1.0 / g.hz;
+  s.t[0] = T(0.5 * (1.0 - r3));
+  s.t[1] = T(0.5 * (1.0 + r3));
+  s.ih[0] = T(1.0 / g.hx);
+  s.ih[1] = T(1.0 / g.hy);
+  s.ih[2] = T(1.0 / g.hz);
   return s;
 }
 
@@ -449,41 +471,42 @@ __device__ __forceinline__ long long nidx(const LevelGeo& g, int i, int j, int k
 
 // Full-weighting restriction of a fine residual at coarse node (fx/2, fy/2, fz/2), neighbours outside
 // the fine grid counted as 0, in the reference's term order (multigrid_intergrid.cpp:124-342).
-__device__ __forceinline__ double full_weight(const LevelGeo& gf, const double* rf, int fx, int fy, int fz) {
+template <typename T>
+__device__ __forceinline__ T full_weight(const LevelGeo& gf, const T* rf, int fx, int fy, int fz) {
   const int Xl = gf.nx - 2, Yl = gf.ny - 2, Zl = gf.nz - 2;
-  auto R = [&](int a, int b, int c) -> double { return rf[nidx(gf, a, b, c)]; };
+  auto R = [&](int a, int b, int c) -> T { return rf[nidx(gf, a, b, c)]; };
   const bool xm = fx < 1, xp = fx > Xl, ym = fy < 1, yq = fy > Yl, zm = fz < 1, zq = fz > Zl;
-  const double r11 = (xm || ym || zm) ? 0.0 : R(fx - 1, fy - 1, fz - 1);
-  const double r12 = (xm || ym || zq) ? 0.0 : R(fx - 1, fy - 1, fz + 1);
-  const double r13 = (xm || yq || zm) ? 0.0 : R(fx - 1, fy + 1, fz - 1);
-  const double r14 = (xm || yq || zq) ? 0.0 : R(fx - 1, fy + 1, fz + 1);
-  const double r15 = (xp || ym || zm) ? 0.0 : R(fx + 1, fy - 1, fz - 1);
-  const double r16 = (xp || ym || zq) ? 0.0 : R(fx + 1, fy - 1, fz + 1);
-  const double r17 = (xp || yq || zm) ? 0.0 : R(fx + 1, fy + 1, fz - 1);
-  const double r18 = (xp || yq || zq) ? 0.0 : R(fx + 1, fy + 1, fz + 1);
-  const double r21 = (xm || ym) ? 0.0 : R(fx - 1, fy - 1, fz);
-  const double r22 = (xm || yq) ? 0.0 : R(fx - 1, fy + 1, fz);
-  const double r23 = (xp || ym) ? 0.0 : R(fx + 1, fy - 1, fz);
-  const double r24 = (xp || yq) ? 0.0 : R(fx + 1, fy + 1, fz);
-  const double r25 = (xm || zm) ? 0.0 : R(fx - 1, fy, fz - 1);
-  const double r26 = (xm || zq) ? 0.0 : R(fx - 1, fy, fz + 1);
-  const double r27 = (xp || zm) ? 0.0 : R(fx + 1, fy, fz - 1);
-  const double r28 = (xp || zq) ? 0.0 : R(fx + 1, fy, fz + 1);
-  const double r29 = (ym || zm) ? 0.0 : R(fx, fy - 1, fz - 1);
-  const double r210 = (ym || zq) ? 0.0 : R(fx, fy - 1, fz + 1);
-  const double r211 = (yq || zm) ? 0.0 : R(fx, fy + 1, fz - 1);
-  const double r212 = (yq || zq) ? 0.0 : R(fx, fy + 1, fz + 1);
-  const double r41 = zm ? 0.0 : R(fx, fy, fz - 1);
-  const double r42 = zq ? 0.0 : R(fx, fy, fz + 1);
-  const double r43 = ym ? 0.0 : R(fx, fy - 1, fz);
-  const double r44 = yq ? 0.0 : R(fx, fy + 1, fz);
-  const double r45 = xm ? 0.0 : R(fx - 1, fy, fz);
-  const double r46 = xp ? 0.0 : R(fx + 1, fy, fz);
-  const double r8 = R(fx, fy, fz);
-  const double s8 = r11 + r12 + r13 + r14 + r15 + r16 + r17 + r18;
-  const double s12 = r21 + r22 + r23 + r24 + r25 + r26 + r27 + r28 + r29 + r210 + r211 + r212;
-  const double s6 = r41 + r42 + r43 + r44 + r45 + r46;
-  return 0.125 * (s8 + 2.0 * s12 + 4.0 * s6 + 8.0 * r8);
+  const T r11 = (xm || ym || zm) ? T(0) : R(fx - 1, fy - 1, fz - 1);
+  const T r12 = (xm || ym || zq) ? T(0) : R(fx - 1, fy - 1, fz + 1);
+  const T r13 = (xm || yq || zm) ? T(0) : R(fx - 1, fy + 1, fz - 1);
+  const T r14 = (xm || yq || zq) ? T(0) : R(fx - 1, fy + 1, fz + 1);
+  const T r15 = (xp || ym || zm) ? T(0) : R(fx + 1, fy - 1, fz - 1);
+  const T r16 = (xp || ym || zq) ? T(0) : R(fx + 1, fy - 1, fz + 1);
+  const T r17 = (xp || yq || zm) ? T(0) : R(fx + 1, fy + 1, fz - 1);
+  const T r18 = (xp || yq || zq) ? T(0) : R(fx + 1, fy + 1, fz + 1);
+  const T r21 = (xm || ym) ? T(0) : R(fx - 1, fy - 1, fz);
+  const T r22 = (xm || yq) ? T(0) : R(fx - 1, fy + 1, fz);
+  const T r23 = (xp || ym) ? T(0) : R(fx + 1, fy - 1, fz);
+  const T r24 = (xp || yq) ? T(0) : R(fx + 1, fy + 1, fz);
+  const T r25 = (xm || zm) ? T(0) : R(fx - 1, fy, fz - 1);
+  const T r26 = (xm || zq) ? T(0) : R(fx - 1, fy, fz + 1);
+  const T r27 = (xp || zm) ? T(0) : R(fx + 1, fy, fz - 1);
+  const T r28 = (xp || zq) ? T(0) : R(fx + 1, fy, fz + 1);
+  const T r29 = (ym || zm) ? T(0) : R(fx, fy - 1, fz - 1);
+  const T r210 = (ym || zq) ? T(0) : R(fx, fy - 1, fz + 1);
+  const T r211 = (yq || zm) ? T(0) : R(fx, fy + 1, fz - 1);
+  const T r212 = (yq || zq) ? T(0) : R(fx, fy + 1, fz + 1);
+  const T r41 = zm ? T(0) : R(fx, fy, fz - 1);
+  const T r42 = zq ? T(0) : R(fx, fy, fz + 1);
+  const T r43 = ym ? T(0) : R(fx, fy - 1, fz);
+  const T r44 = yq ? T(0) : R(fx, fy + 1, fz);
+  const T r45 = xm ? T(0) : R(fx - 1, fy, fz);
+  const T r46 = xp ? T(0) : R(fx + 1, fy, fz);
+  const T r8 = R(fx, fy, fz);
+  const T s8 = r11 + r12 + r13 + r14 + r15 + r16 + r17 + r18;
+  const T s12 = r21 + r22 + r23 + r24 + r25 + r26 + r27 + r28 + r29 + r210 + r211 + r212;
+  const T s6 = r41 + r42 + r43 + r44 + r45 + r46;
+  return T(0.125) * (s8 + T(2) * s12 + T(4) * s6 + T(8) * r8);
 }
 
 }  // namespace hpc

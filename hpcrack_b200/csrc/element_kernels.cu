@@ -5,8 +5,9 @@
 // nodes), wy element rows in y (wy-1 output node rows) and cz output node planes in z, and
 // streams it row by row, layer by layer.  The strip shape (wy, cz) is chosen per level: long strips
 // on large levels (little recomputation at strip edges), short ones on small levels, where the
-// serial chain of elements a warp computes would otherwise set the kernel's duration.  Node rows are staged into a per-warp shared-memory ring
-// with cp.async two rows ahead of use, so global-memory latency never sits on the element math.
+// serial chain of elements a warp computes would otherwise set the kernel's duration.  Node rows
+// are staged into a per-warp shared-memory ring with cp.async two rows ahead of use, so
+// global-memory latency never sits on the element math.
 // Per row step a lane computes one element from the staged rows; x-neighbour contributions are
 // combined with one shuffle, y-neighbours through registers (the previous row's upper-face sums)
 // and z-neighbours through a per-warp shared-memory carry of the previous layer's upper faces.
@@ -45,16 +46,30 @@ inline StripGeo strip_geo(const LevelGeo& g, int wy, int cz) {
   return s;
 }
 
-// The longest strip shape that still gives every resident warp slot about two strips; small
-// levels end at 2 x 2 (one output row, two output planes per warp).
-inline StripGeo choose_strips(const LevelGeo& g, long long warp_slots) {
-  static const int shapes[][2] = {{8, 16}, {8, 8}, {4, 8}, {4, 4}, {2, 4}, {2, 2}};
-  StripGeo s{};
-  for (const auto& sh : shapes) {
-    s = strip_geo(g, sh[0], sh[1]);
-    if (s.nstrips >= 2 * warp_slots) break;
-  }
-  return s;
+// Strip shape of a level by a latency model of the element math: the FP64 unit of an SM
+// sub-partition finishes one element per fixed time whether one or several warps feed it, so a
+// level's duration is set by the longest chain of elements one sub-partition computes,
+//   wy * (cz + 1) elements per strip  x  ceil(strips / sub-partitions).
+// Short strips shorten the chain but recompute more strip-edge elements; the model picks the
+// shape with the shortest chain (ties: the least recomputation).
+inline StripGeo choose_strips(const LevelGeo& g, long long subpartitions) {
+  static const int wys[] = {8, 4, 2};
+  static const int czs[] = {32, 16, 8, 4, 2};
+  StripGeo best{};
+  long long best_chain = -1, best_work = 0;
+  for (int wy : wys)
+    for (int cz : czs) {
+      const StripGeo s = strip_geo(g, wy, cz);
+      const long long per = (long long)wy * (cz + 1);
+      const long long chain = per * ((s.nstrips + subpartitions - 1) / subpartitions);
+      const long long work = per * s.nstrips;
+      if (best_chain < 0 || chain < best_chain || (chain == best_chain && work < best_work)) {
+        best = s;
+        best_chain = chain;
+        best_work = work;
+      }
+    }
+  return best;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -65,16 +80,23 @@ __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool
   const int sz = pred ? 8 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
 }
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = pred ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_el(double* smem, const double* gmem, bool pred) { cp_async8(smem, gmem, pred); }
+__device__ __forceinline__ void cp_async_el(float* smem, const float* gmem, bool pred) { cp_async4(smem, gmem, pred); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::: "memory"); }
 
 // A strip's staged stream: for each layer kk = z0-1 .. zend, node rows y = y0-1 .. y0-1+wy
 // (rows = wy+1 rows), each row holding NF fields on the two planes kk and kk+1.  Stream row s sits in
 // ring slot s % kRing at ring[((slot*NF + f)*2 + c)*kRowW + lane].
-template <int NF>
+template <int NF, typename T = double>
 struct Stream {
-  double* ring;
-  const double* const* fields;  // NF global arrays (node-indexed)
+  T* ring;
+  const T* const* fields;  // NF global arrays (node-indexed)
   int x, y0, z0, nlayers, total, rows;
   const LevelGeo* g;
 
@@ -89,12 +111,12 @@ struct Stream {
         const bool ok = x >= 0 && x < g->nx && y >= 0 && y < g->ny && z >= 0 && z < g->nz;
         const long long n = ok ? (long long)x + (long long)y * g->px + (long long)z * g->plane : 0;
 #pragma unroll
-        for (int f = 0; f < NF; ++f) cp_async8(ring + ((slot * NF + f) * 2 + c) * kRowW + lane, fields[f] + n, ok);
+        for (int f = 0; f < NF; ++f) cp_async_el(ring + ((slot * NF + f) * 2 + c) * kRowW + lane, fields[f] + n, ok);
       }
     }
     cp_async_commit();
   }
-  __device__ __forceinline__ double at(int s, int f, int c, int col) const {
+  __device__ __forceinline__ T at(int s, int f, int c, int col) const {
     return ring[(((s & (kRing - 1)) * NF + f) * 2 + c) * kRowW + col];
   }
 };
@@ -102,27 +124,40 @@ struct Stream {
 // ------------------------------------------------------------------------------------------
 // mechanical
 // ------------------------------------------------------------------------------------------
-struct MechK {
+template <typename T>
+struct MechKT {
   LevelGeo g;
   LevelGeo gf;  // fine level (FAS)
   StripGeo sg;
-  const double* fields[6];  // staged: u0,u1,u2 then K,G,d (finest) or Ke,Ge (coarse)
-  double* out;
+  const T* fields[6];  // staged: u0,u1,u2 then K,G,d (finest) or Ke,Ge (coarse)
+  T* out;
   const int8_t* choice;
   double small_k;
-  double* fu;
+  T* fu;
   int set_fnorm;
-  const double* invM;
-  const double* rf;
+  const T* invM;
+  const T* rf;
   RedTarget red;
 };
+using MechK = MechKT<double>;
+
+// d clamped to [0, 1] (K_G_d_g, material_gauss_point.cpp:51-54), decided on the bit pattern:
+// negative values (sign bit set) give 0, values above 1 give 1.
+__device__ __forceinline__ double clamp01(double v) {
+  const long long b = __double_as_longlong(v);
+  return b < 0 ? 0.0 : (b > 0x3FF0000000000000LL ? 1.0 : v);
+}
+__device__ __forceinline__ float clamp01(float v) {
+  const int b = __float_as_int(v);
+  return b < 0 ? 0.0f : (b > 0x3F800000 ? 1.0f : v);
+}
 
 // Per-Gauss-point moduli times wg (MP_all_GAUSS_Point, mechanical_pcg.cpp:26-61), finest level:
 // trilinear nodal K, G, d with the zero rule, clamp and degradation by regime.
-__device__ __forceinline__ void mech_moduli_finest(const double (&Kn)[8], const double (&Gn)[8], const double (&dn)[8],
-                                                   int ch, double small_k, double wg, const SF& s, double (&Kw)[8],
-                                                   double (&Gw)[8]) {
-  double Kg[8], Gg[8];
+template <typename T>
+__device__ __forceinline__ void mech_moduli_finest(const T (&Kn)[8], const T (&Gn)[8], const T (&dn)[8], int ch,
+                                                   T small_k, T wg, const SFt<T>& s, T (&Kw)[8], T (&Gw)[8]) {
+  T Kg[8], Gg[8];
   gp_material(Kn, s, Kg);
   gp_material(Gn, s, Gg);
   if (ch == 2) {
@@ -132,31 +167,32 @@ __device__ __forceinline__ void mech_moduli_finest(const double (&Kn)[8], const 
       Gw[g] = Gg[g] * wg;
     }
   } else {
-    double dg[8];
+    T dg[8];
     gp_material(dn, s, dg);
+    const T one_k = T(1) - small_k;
 #pragma unroll
     for (int g = 0; g < 8; ++g) {
-      const double dd = fmin(fmax(dg[g], 0.0), 1.0);  // K_G_d_g clamp (material_gauss_point.cpp:51-54)
-      const double om = 1.0 - dd;
-      const double gd = fma((1.0 - small_k) * om, om, small_k);
+      const T om = T(1) - clamp01(dg[g]);
+      const T gd = fma(one_k * om, om, small_k);
       Kw[g] = (ch == 0 ? gd * Kg[g] : Kg[g]) * wg;
       Gw[g] = (gd * Gg[g]) * wg;
     }
   }
 }
 
-template <bool FINEST, int EPI, bool DIAG>
-__global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
+// T = double: the plain form; T = float: the precision form's V-cycle (reductions stay FP64).
+template <typename T, bool FINEST, int EPI, bool DIAG, bool ISO>
+__global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
   constexpr int NU = DIAG ? 0 : 3;
   constexpr int NF = NU + (FINEST ? 3 : 2);
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) unsigned char mech_smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  double* ring = smem + (size_t)wib * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32);
-  double* zc = ring + kRing * NF * 2 * kRowW;  // [row][comp][lane]
-  const SF s = make_sf(k.g);
+  T* ring = reinterpret_cast<T*>(mech_smem) + (size_t)wib * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32);
+  T* zc = ring + kRing * NF * 2 * kRowW;  // [row][comp][lane]
+  const SFt<T> s = make_sf<T>(k.g);
   double red0 = 0.0, red1 = 0.0, red2 = 0.0;
   const long long nwarps_total = (long long)gridDim.x * kWarps;
-  const double* fptr[NF];
+  const T* fptr[NF];
 #pragma unroll
   for (int f = 0; f < NF; ++f) fptr[f] = k.fields[f];
 
@@ -169,11 +205,11 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
     const int x0 = sx * kOX, y0 = sy * (wy - 1), z0 = sz * k.sg.cz;
     const int x = x0 - 1 + lane;
     const int zend = min(z0 + k.sg.cz - 1, k.g.nz - 1);
-    Stream<NF> st{ring, fptr, x, y0, z0, zend - z0 + 2, 0, rows, &k.g};
+    Stream<NF, T> st{ring, fptr, x, y0, z0, zend - z0 + 2, 0, rows, &k.g};
     st.total = st.nlayers * rows;
     st.issue(0, lane);
     st.issue(1, lane);
-    double yp[2][3];
+    T yp[2][3];
     for (int si = 0; si < st.total; ++si) {
       st.issue(si + 2, lane);
       cp_async_wait2();
@@ -184,20 +220,21 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
 #pragma unroll
         for (int c = 0; c < 2; ++c)
 #pragma unroll
-          for (int m = 0; m < 3; ++m) yp[c][m] = 0.0;
+          for (int m = 0; m < 3; ++m) yp[c][m] = T(0);
         __syncwarp();
         continue;
       }
       const int rr = r - 1, ey = y0 - 1 + rr;
       // ---- element (x, ey, kk) from stream rows si-1 (y = ey) and si (y = ey+1)
-      double f[3][8];
+      T f[3][8];
       const bool valid = lane < 31 && x >= 0 && x <= k.g.nx - 2 && ey >= 0 && ey <= k.g.ny - 2 && kk >= 0 &&
                          kk <= k.g.nz - 2;
       if (valid) {
-        double Kw[8], Gw[8];
-        const double wg = k.g.wg;
+        T Kw[8], Gw[8];
+        // ISO: the 1/h^2 of the two gradients goes into the Gauss weight (see sf_forward)
+        const T wg = ISO ? T(k.g.wg) * (s.ih[0] * s.ih[0]) : T(k.g.wg);
         if (FINEST) {
-          double Kn[8], Gn[8], dn[8];
+          T Kn[8], Gn[8], dn[8];
 #pragma unroll
           for (int n = 0; n < 8; ++n) {
             const int a = n & 1, b = (n >> 1) & 1, c = n >> 2;
@@ -207,19 +244,19 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
             dn[n] = st.at(srow, NU + 2, c, lane + a);
           }
           const long long e = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
-          mech_moduli_finest(Kn, Gn, dn, k.choice[e], k.small_k, wg, s, Kw, Gw);
+          mech_moduli_finest(Kn, Gn, dn, k.choice[e], T(k.small_k), wg, s, Kw, Gw);
         } else {
-          const double K = st.at(si - 1, NU + 0, 0, lane) * wg, G = st.at(si - 1, NU + 1, 0, lane) * wg;
+          const T K = st.at(si - 1, NU + 0, 0, lane) * wg, G = st.at(si - 1, NU + 1, 0, lane) * wg;
 #pragma unroll
           for (int g = 0; g < 8; ++g) {
             Kw[g] = K;
             Gw[g] = G;
           }
         }
-        if (DIAG) {
+        if constexpr (DIAG) {
           mech_element_diag(Kw, Gw, s, f);
         } else {
-          double u[3][8];
+          T u[3][8];
 #pragma unroll
           for (int n = 0; n < 8; ++n) {
             const int a = n & 1, b = (n >> 1) & 1, c = n >> 2;
@@ -227,31 +264,31 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
 #pragma unroll
             for (int m = 0; m < 3; ++m) u[m][n] = st.at(srow, m, c, lane + a);
           }
-          mech_element(u, Kw, Gw, s, f);
+          mech_element<ISO>(u, Kw, Gw, s, f);
         }
       } else {
 #pragma unroll
         for (int m = 0; m < 3; ++m)
 #pragma unroll
-          for (int n = 0; n < 8; ++n) f[m][n] = 0.0;
+          for (int n = 0; n < 8; ++n) f[m][n] = T(0);
       }
       // ---- combine x-neighbours: node x gets own a=0 corners + left lane's a=1 corners
-      double X[2][2][3];  // [b][c][m]
+      T X[2][2][3];  // [b][c][m]
 #pragma unroll
       for (int c = 0; c < 2; ++c)
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
           for (int m = 0; m < 3; ++m) {
-            const double left = __shfl_up_sync(kFull, f[m][1 + 2 * b + 4 * c], 1);
-            X[b][c][m] = f[m][2 * b + 4 * c] + (lane > 0 ? left : 0.0);
+            const T left = __shfl_up_sync(kFull, f[m][1 + 2 * b + 4 * c], 1);
+            X[b][c][m] = f[m][2 * b + 4 * c] + (lane > 0 ? left : T(0));
           }
       if (rr >= 1) {
         const int orow = rr - 1;
-        double tot[3];
+        T tot[3];
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-          double* zp = zc + (orow * 3 + m) * 32 + lane;
+          T* zp = zc + (orow * 3 + m) * 32 + lane;
           tot[m] = *zp + yp[0][m] + X[0][0][m];
           *zp = yp[1][m] + X[0][1][m];
         }
@@ -266,22 +303,22 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechK k) {
             const bool fix[3] = {bc.c0, bc.c1, bc.c2};
 #pragma unroll
             for (int m = 0; m < 3; ++m) {
-              double fv = k.fu[n + m * N];
+              T fv = k.fu[n + m * N];
               if (k.set_fnorm && fix[m]) {
                 fv = tot[m];
                 k.fu[n + m * N] = fv;
               }
-              red0 = fma(fv, fv, red0);
-              const double rv = fix[m] ? 0.0 : fv - tot[m];
+              red0 = fma((double)fv, (double)fv, red0);
+              const T rv = fix[m] ? T(0) : fv - tot[m];
               k.out[n + m * N] = rv;
-              if (k.invM) red1 = fma(rv, rv * k.invM[n + m * N], red1);
-              red2 = fma(rv, rv, red2);
+              if (k.invM) red1 = fma((double)rv, (double)(rv * k.invM[n + m * N]), red1);
+              red2 = fma((double)rv, (double)rv, red2);
             }
           } else if (EPI == EPI_PCG) {  // w = K p, (p, w)
 #pragma unroll
             for (int m = 0; m < 3; ++m) {
               k.out[n + m * N] = tot[m];
-              red0 = fma(st.at(si - 1, m, 0, lane), tot[m], red0);
+              red0 = fma((double)st.at(si - 1, m, 0, lane), (double)tot[m], red0);
             }
           } else if (EPI == EPI_FAS) {
             // coarsen_f_standard_routine (multigrid_intergrid.cpp:124-342) fused with the coarse apply
@@ -374,7 +411,7 @@ static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls) {
   const int rc = kernel_cfg(kern, smem, &per_sm);
   if (rc) return rc;
   const long long cap = (long long)num_sms() * per_sm;
-  a.sg = choose_strips(a.g, cap * kWarps);
+  a.sg = choose_strips(a.g, (long long)num_sms() * 4);
   const StripGeo& sg = a.sg;
   const long long need = (sg.nstrips + kWarps - 1) / kWarps;
   const int grid = (int)(need < cap ? need : cap);
@@ -387,12 +424,18 @@ static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls) {
   return HPC_OK;
 }
 
-template <bool F, int E, bool D>
-static int run_mech(hpc_ctx* c, const MechK& k) {
+// Isotropic spacing (hx = hy = hz) selects the kernels that fold 1/h^2 into the material.
+inline bool iso(const LevelGeo& g) { return g.hx == g.hy && g.hy == g.hz; }
+
+template <bool F, int E, bool D, typename T = double>
+static int run_mech(hpc_ctx* c, const MechKT<T>& k) {
   constexpr int NF = (D ? 0 : 3) + (F ? 3 : 2);
-  const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(double);
-  const int cls = (F && E == EPI_PCG && !D) ? HPC_KC_MECH_PCG_FINEST : HPC_KC_NONE;
-  return launch_strips(c, mech_kernel<F, E, D>, k, smem, cls);
+  const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
+  const int cls = (F && E == EPI_PCG && !D && sizeof(T) == 8) ? HPC_KC_MECH_PCG_FINEST : HPC_KC_NONE;
+  if constexpr (!D) {
+    if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true>, k, smem, cls);
+  }
+  return launch_strips(c, mech_kernel<T, F, E, D, false>, k, smem, cls);
 }
 
 static void mech_fields(hpc_ctx* c, int level, bool finest, bool diag, const double* src, MechK& k) {
@@ -449,6 +492,45 @@ int launch_mech_diag(hpc_ctx* c, int level, bool finest, double small_k, double*
   return finest ? run_mech<true, EPI_PLAIN, true>(c, k) : run_mech<false, EPI_PLAIN, true>(c, k);
 }
 
+// Single-precision element operator of the precision form's V-cycle: the same kernels on the FP32
+// mirror of a level (LevelF32); residual, PCG apply and FAS right-hand side epilogues.
+int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
+  MechKT<float> k{};
+  const LevelF32& F = c->F32[m.level];
+  const LevelGeo& g = c->L[m.level];
+  k.g = g;
+  if (m.epi == EPI_FAS) k.gf = c->L[m.fine_level];
+  int f = 0;
+  for (int q = 0; q < 3; ++q) k.fields[f++] = m.src + (long long)q * g.n;
+  if (m.finest) {
+    k.fields[f++] = F.K;
+    k.fields[f++] = F.G;
+    k.fields[f++] = F.d;
+  } else {
+    k.fields[f++] = F.Ke;
+    k.fields[f++] = F.Ge;
+  }
+  for (; f < 6; ++f) k.fields[f] = k.fields[3];
+  k.out = m.out;
+  k.choice = c->F[m.level].choice;
+  k.small_k = m.small_k;
+  k.fu = m.fu;
+  k.set_fnorm = 0;
+  k.invM = m.invM;
+  k.rf = m.rf;
+  k.red = make_red(c, m.s_out0, m.s_out1, m.s_out2);
+  const bool fin = m.finest;
+  switch (m.epi) {
+    case EPI_PLAIN:
+      return fin ? run_mech<true, EPI_PLAIN, false>(c, k) : run_mech<false, EPI_PLAIN, false>(c, k);
+    case EPI_RESIDUAL:
+      return fin ? run_mech<true, EPI_RESIDUAL, false>(c, k) : run_mech<false, EPI_RESIDUAL, false>(c, k);
+    case EPI_PCG: return fin ? run_mech<true, EPI_PCG, false>(c, k) : run_mech<false, EPI_PCG, false>(c, k);
+    case EPI_FAS: return run_mech<false, EPI_FAS, false>(c, k);
+  }
+  return HPC_ERR_ARG;
+}
+
 // ------------------------------------------------------------------------------------------
 // phase field
 // ------------------------------------------------------------------------------------------
@@ -464,7 +546,7 @@ struct PfK {
   RedTarget red;
 };
 
-template <int EPI, bool DIAG>
+template <int EPI, bool DIAG, bool ISO>
 __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
   constexpr int NF = 3;
   extern __shared__ double smem[];
@@ -474,7 +556,8 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
   const SF s = make_sf(k.g);
   double red0 = 0.0, red1 = 0.0, red2 = 0.0;
   const long long nwarps_total = (long long)gridDim.x * kWarps;
-  const double wg = k.g.wg, inv_lc = 1.0 / k.lc;
+  // ISO: only the gradient term carries 1/h^2 (see sf_forward); the mass term keeps wg
+  const double wg = k.g.wg, wgb = ISO ? k.g.wg * (s.ih[0] * s.ih[0]) : k.g.wg, inv_lc = 1.0 / k.lc;
   const double* fptr[NF] = {k.fields[0], k.fields[1], k.fields[2]};
 
   for (long long strip = (long long)blockIdx.x * kWarps + wib; strip < k.sg.nstrips; strip += nwarps_total) {
@@ -518,7 +601,7 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
 #pragma unroll
         for (int g = 0; g < 8; ++g) {
           aw[g] = wg * fma(gcg[g], inv_lc, H2);
-          bw[g] = wg * (gcg[g] * k.lc);
+          bw[g] = wgb * (gcg[g] * k.lc);
         }
         if (DIAG) {
           pf_element_diag(aw, bw, s, f);
@@ -529,7 +612,7 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
             const int a = n & 1, b = (n >> 1) & 1, c = n >> 2;
             xv[n] = st.at(b ? si : si - 1, 0, c, lane + a);
           }
-          pf_element(xv, aw, bw, s, f);
+          pf_element<ISO>(xv, aw, bw, s, f);
         }
       } else {
 #pragma unroll
@@ -581,7 +664,10 @@ template <int E, bool D>
 static int run_pf(hpc_ctx* c, const PfK& k, bool finest) {
   const size_t smem = (size_t)kWarps * (kRing * 3 * 2 * kRowW + (kWY - 1) * 32) * sizeof(double);
   const int cls = (finest && E == EPI_PCG && !D) ? HPC_KC_PF_PCG_FINEST : HPC_KC_NONE;
-  return launch_strips(c, pf_kernel<E, D>, k, smem, cls);
+  if constexpr (!D) {
+    if (iso(k.g)) return launch_strips(c, pf_kernel<E, D, true>, k, smem, cls);
+  }
+  return launch_strips(c, pf_kernel<E, D, false>, k, smem, cls);
 }
 
 int launch_pf(hpc_ctx* c, const PfCall& p) {

@@ -499,6 +499,271 @@ static int u_entire_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut,
   return launch_mech(c, r);
 }
 
+// ---------------------------------------------------------------- precision form: FP32 V-cycle
+// The preconditioner of the mixed-precision solve: one V-cycle of cycle_u's kind (restarted
+// Jacobi-PCG smoothing, injection, FAS right-hand side, prolongation) on single-precision copies of
+// the levels, solving for a correction (homogeneous Dirichlet values).  Its coarsest solve stays FP64.
+static int ensure_f32(hpc_ctx* c) {
+  if (c->F32[0].u) return HPC_OK;
+  for (int l = 0; l <= c->maxlevel; ++l) {
+    const size_t n = (size_t)c->L[l].n;
+    LevelF32& F = c->F32[l];
+    float** vec[] = {&F.u, &F.fu, &F.ru, &F.uold, &F.p, &F.w, &F.invM};
+    for (float** p : vec) {
+      HPC_CUDA(cudaMalloc((void**)p, 3 * n * sizeof(float)));
+      HPC_CUDA(cudaMemsetAsync(*p, 0, 3 * n * sizeof(float), c->stream));
+    }
+    float** mat_f[] = {&F.K, &F.G, &F.d};
+    float** mat_c[] = {&F.Ke, &F.Ge};
+    const bool fin = (l == c->maxlevel);
+    for (int q = 0; q < (fin ? 3 : 2); ++q) {
+      float** p = fin ? mat_f[q] : mat_c[q];
+      HPC_CUDA(cudaMalloc((void**)p, n * sizeof(float)));
+      HPC_CUDA(cudaMemsetAsync(*p, 0, n * sizeof(float), c->stream));
+    }
+  }
+  return HPC_OK;
+}
+
+// FP32 material and inverse diagonals from the FP64 ones (after mech_material and mech_diags).
+static int f32_material(hpc_ctx* c) {
+  int rc;
+  for (int l = 0; l <= c->maxlevel; ++l) {
+    const long long n = c->L[l].n;
+    LevelF32& G = c->F32[l];
+    const LevelFields& F = c->F[l];
+    if ((rc = launch_to_f32(c, F.preMu, G.invM, 3 * n))) return rc;
+    if (l == c->maxlevel) {
+      if ((rc = launch_to_f32(c, F.bulK, G.K, n))) return rc;
+      if ((rc = launch_to_f32(c, F.G, G.G, n))) return rc;
+      if ((rc = launch_to_f32(c, F.d, G.d, n))) return rc;
+    } else {
+      if ((rc = launch_to_f32(c, F.Ke, G.Ke, n))) return rc;
+      if ((rc = launch_to_f32(c, F.Ge, G.Ge, n))) return rc;
+    }
+  }
+  return HPC_OK;
+}
+
+// pcg_u (mechanical_pcg.cpp:223-330) on the FP32 mirror, homogeneous Dirichlet values.
+static int pcg_u32(hpc_ctx* c, int l, double small_k, int nb) {
+  if (nb > kMaxRelax) return arg_fail("nb_relax too large");
+  LevelF32& F = c->F32[l];
+  int rc;
+  if ((rc = launch_bc_zero_f32(c, l, F.u))) return rc;
+  MechCall32 m{};
+  m.level = l;
+  m.finest = is_finest(c, l);
+  m.epi = EPI_RESIDUAL;
+  m.src = F.u;
+  m.out = F.ru;
+  m.small_k = small_k;
+  m.fu = F.fu;
+  m.invM = F.invM;
+  m.s_out0 = -1;
+  m.s_out1 = slot_rz(0);
+  m.s_out2 = -1;
+  if ((rc = launch_mech_f32(c, m))) return rc;
+  for (int it = 0; it < nb; ++it) {
+    if ((rc = launch_dir_update_f32(c, l, it == 0, slot_rz(it), slot_rz(it - 1)))) return rc;
+    MechCall32 q{};
+    q.level = l;
+    q.finest = m.finest;
+    q.epi = EPI_PCG;
+    q.src = F.p;
+    q.out = F.w;
+    q.small_k = small_k;
+    q.s_out0 = slot_pw(it);
+    q.s_out1 = q.s_out2 = -1;
+    if ((rc = launch_mech_f32(c, q))) return rc;
+    if ((rc = launch_mech_update_f32(c, l, slot_rz(it), slot_pw(it), slot_rz(it + 1), slot_rn(it)))) return rc;
+  }
+  return HPC_OK;
+}
+
+// The coarsest level in FP64: pcg_u with nu0 iterations on the FP64 arrays of level 0.
+static int coarsest64(hpc_ctx* c, const hpc_mg& mg, double small_k) {
+  const long long n3 = 3 * c->L[0].n;
+  int rc;
+  if ((rc = launch_to_f64(c, c->F32[0].u, c->F[0].u, n3))) return rc;
+  if ((rc = launch_to_f64(c, c->F32[0].fu, c->F[0].fu, n3))) return rc;
+  if ((rc = pcg_u_dev(c, 0, small_k, 0.0, mg.nu0, 1))) return rc;
+  return launch_to_f32(c, c->F[0].u, c->F32[0].u, n3);
+}
+
+static int cycle_u32(hpc_ctx* c, int l, const hpc_mg& mg, double small_k);
+
+static int coarse_part_u32(hpc_ctx* c, int l, const hpc_mg& mg, double small_k) {
+  int rc;
+  if ((rc = launch_inject_u_f32(c, l))) return rc;
+  MechCall32 f{};
+  f.level = l - 1;
+  f.finest = false;
+  f.epi = EPI_FAS;
+  f.src = c->F32[l - 1].u;
+  f.out = c->F32[l - 1].fu;
+  f.small_k = small_k;
+  f.rf = c->F32[l].ru;
+  f.fine_level = l;
+  f.s_out0 = f.s_out1 = f.s_out2 = -1;
+  if ((rc = launch_mech_f32(c, f))) return rc;
+  for (int j = 1; j <= mg.gamma; ++j)
+    if ((rc = cycle_u32(c, l - 1, mg, small_k))) return rc;
+  return launch_prolong_f32(c, l);
+}
+
+static int cycle_u32(hpc_ctx* c, int l, const hpc_mg& mg, double small_k) {
+  int rc;
+  if (l == 0) return coarsest64(c, mg, small_k);
+  if ((rc = pcg_u32(c, l, small_k, mg.nu1))) return rc;
+  if ((rc = coarse_part_u32(c, l, mg, small_k))) return rc;
+  return pcg_u32(c, l, small_k, mg.nu2);
+}
+
+// ---------------------------------------------------------------- flexible PCG (precision form)
+static int ensure_fcg(hpc_ctx* c) {
+  if (c->fcg.x) return HPC_OK;
+  const size_t bytes = sizeof(double) * 3 * (size_t)c->L[c->maxlevel].n;
+  double** arrs[] = {&c->fcg.x, &c->fcg.r, &c->fcg.rp, &c->fcg.f, &c->fcg.p};
+  for (double** a : arrs) {
+    HPC_CUDA(cudaMalloc((void**)a, bytes));
+    HPC_CUDA(cudaMemsetAsync(*a, 0, bytes, c->stream));
+  }
+  return HPC_OK;
+}
+
+// True residual r = f - K x with Dirichlet rows zero; at t == 0 the reactions of x become f's
+// Dirichlet rows and f_norm (as every finest pcg_u call at t == 0 does, mechanical_pcg.cpp:252-258).
+static int fcg_residual(hpc_ctx* c, double small_k, int t, int s_rn) {
+  const int L = c->maxlevel;
+  MechCall m{};
+  m.level = L;
+  m.finest = true;
+  m.epi = EPI_RESIDUAL;
+  m.src = c->fcg.x;
+  m.out = c->fcg.r;
+  m.small_k = small_k;
+  m.fu = c->fcg.f;
+  m.set_fnorm = (t == 0);
+  m.invM = nullptr;
+  m.s_out0 = m.set_fnorm ? S_FNORM : -1;
+  m.s_out1 = -1;
+  m.s_out2 = s_rn;
+  return launch_mech(c, m);
+}
+
+// The mechanical solve of u_entire (mechanical_displacement.cpp:25-115) by flexible PCG on the finest
+// level, preconditioned by one multigrid V-cycle of the reference's kind (FAS with restarted
+// Jacobi-PCG smoothers, which on the linear correction problem acts as a correction-scheme cycle).
+// The outer iteration keeps the true residual, the dot products and the x / r / p updates in FP64;
+// the stopping test is the reference's |r|^2 / |f|^2 <= mech_tol.  *cycles = V-cycles (one per
+// iteration), *fin_iters = finest smoother iterations inside them.
+static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, double mech_tol,
+                            int* cycles, long long* fin_iters, bool mixed) {
+  int rc;
+  const int L = c->maxlevel;
+  LevelFields& F = c->F[L];
+  const LevelGeo& g = c->L[L];
+  const size_t vbytes = sizeof(double) * 3 * (size_t)g.n;
+  if ((rc = ensure_fcg(c))) return rc;
+  if (mg.ncy + 1 > kMaxRelax) return arg_fail("ncy too large");
+  if ((rc = write_scalar(c, S_FNORM, c->f_norm))) return rc;
+  if ((rc = mech_material(c, small_k))) return rc;
+  if ((rc = mech_diags(c, L, small_k))) return rc;
+  if (mixed) {
+    if ((rc = ensure_f32(c))) return rc;
+    if ((rc = f32_material(c))) return rc;
+  }
+  // x = u with the Dirichlet values, f = fu (saved: the V-cycle uses fu as its right-hand side)
+  if ((rc = launch_bc(c, L, F.u, nullptr, 0, Ut))) return rc;
+  HPC_CUDA(cudaMemcpyAsync(c->fcg.x, F.u, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+  HPC_CUDA(cudaMemcpyAsync(c->fcg.f, F.fu, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+  if ((rc = fcg_residual(c, small_k, t, slot_frn(-1)))) return rc;
+  double s2[2];
+  if ((rc = read_scalars(c, S_FNORM, 1, s2))) return rc;
+  if ((rc = read_scalars(c, slot_frn(-1), 1, s2 + 1))) return rc;
+  double f_norm = s2[0], rel = f_norm != 0 ? s2[1] / f_norm : 1.0;
+  *cycles = 0;
+  *fin_iters = 0;
+  const int per_cycle = (L == 0) ? mg.nu0 : mg.nu1 + mg.nu2;
+  for (int k = 0; k < mg.ncy; ++k) {
+    if (rel <= mech_tol && !(t == 0 && k == 0)) break;  // one iteration forced at t == 0 (:74, :84-85)
+    // z = V-cycle on A z = r from z = 0 with homogeneous Dirichlet values: u is the cycle's unknown,
+    // fu its right-hand side
+    if (mixed) {  // the same cycle on the FP32 mirror; z comes back to F.u in FP64
+      const LevelF32& G = c->F32[L];
+      HPC_CUDA(cudaMemsetAsync(G.u, 0, 3 * (size_t)g.n * sizeof(float), c->stream));
+      if ((rc = launch_to_f32(c, c->fcg.r, G.fu, 3 * g.n))) return rc;
+      if (L == 0) {
+        if ((rc = cycle_u32(c, 0, mg, small_k))) return rc;
+      } else {
+        if ((rc = pcg_u32(c, L, small_k, mg.nu1))) return rc;
+        if ((rc = run_graphed(c, c->g32, mg, small_k, 0.0, k > 0,
+                              [&] { return coarse_part_u32(c, L, mg, small_k); })))
+          return rc;
+        if ((rc = pcg_u32(c, L, small_k, mg.nu2))) return rc;
+      }
+      if ((rc = launch_to_f64(c, G.u, F.u, 3 * g.n))) return rc;
+    } else {
+      HPC_CUDA(cudaMemsetAsync(F.u, 0, vbytes, c->stream));
+      HPC_CUDA(cudaMemcpyAsync(F.fu, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+      if ((rc = cycle_u_top(c, mg, small_k, 0.0, 1, k > 0))) return rc;
+    }
+    ++*cycles;
+    *fin_iters += per_cycle;
+    // delta_k = (z, r_k), gamma_k = (z, r_{k-1}); p = z + beta p
+    if ((rc = launch_dot2(c, L, F.u, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k)))) return rc;
+    if ((rc = launch_fcg_dir(c, L, F.u, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
+      return rc;
+    // w = K p, (p, w); the smoothers' own p and w are free between V-cycles
+    MechCall q{};
+    q.level = L;
+    q.finest = true;
+    q.epi = EPI_PCG;
+    q.src = c->fcg.p;
+    q.out = F.w;
+    q.small_k = small_k;
+    q.s_out0 = slot_fpw(k);
+    q.s_out1 = q.s_out2 = -1;
+    if ((rc = launch_mech(c, q))) return rc;
+    // r_{k-1} kept for the flexible beta; x += alpha p, r -= alpha w, alpha = delta_k / (p, w)
+    HPC_CUDA(cudaMemcpyAsync(c->fcg.rp, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = launch_mech_update_on(c, L, c->fcg.x, c->fcg.r, c->fcg.p, F.w, F.preMu, slot_fdelta(k), slot_fpw(k),
+                                    slot_fdummy(k), slot_frn(k))))
+      return rc;
+    // The stopping decision is always taken on the true residual f - K x: at t == 0 it is computed
+    // every iteration (f_norm follows the reactions of the current iterate); later the recursive
+    // residual is used until it passes the test, then the true one confirms it or replaces it.
+    double rn;
+    if (t == 0) {
+      if ((rc = fcg_residual(c, small_k, t, slot_frn(k)))) return rc;
+      if ((rc = read_scalars(c, S_FNORM, 1, &f_norm))) return rc;
+      if ((rc = read_scalars(c, slot_frn(k), 1, &rn))) return rc;
+    } else {
+      if ((rc = read_scalars(c, slot_frn(k), 1, &rn))) return rc;
+      if (f_norm != 0 && rn / f_norm <= mech_tol) {
+        if ((rc = fcg_residual(c, small_k, t, slot_frn(k)))) return rc;
+        if ((rc = read_scalars(c, slot_frn(k), 1, &rn))) return rc;
+      }
+    }
+    rel = f_norm != 0 ? rn / f_norm : 1.0;
+  }
+  c->f_norm = f_norm;
+  // u = x, fu restored; externe_force_nodal (mechanical_right_hnd.cpp:18-38)
+  HPC_CUDA(cudaMemcpyAsync(F.u, c->fcg.x, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+  HPC_CUDA(cudaMemcpyAsync(F.fu, c->fcg.f, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+  if ((rc = launch_bc(c, L, F.u, nullptr, 0, Ut))) return rc;
+  MechCall r{};
+  r.level = L;
+  r.finest = true;
+  r.epi = EPI_REACTION;
+  r.src = F.u;
+  r.out = F.fu;
+  r.small_k = small_k;
+  r.s_out0 = r.s_out1 = r.s_out2 = -1;
+  return launch_mech(c, r);
+}
+
 // phase_field (phase_field.cpp:15-57).
 static int phase_field_dev(hpc_ctx* c, const hpc_mg& mg, double lc, double pf_tol, int* cycles, long long* fin_iters) {
   int rc;
@@ -716,6 +981,18 @@ int hpc_destroy(hpc_ctx* c) {
   delete[] c->tev;
   if (c->gmech.valid) cudaGraphExecDestroy(c->gmech.exec);
   if (c->gpf.valid) cudaGraphExecDestroy(c->gpf.exec);
+  {
+    double* fa[] = {c->fcg.x, c->fcg.r, c->fcg.rp, c->fcg.f, c->fcg.p};
+    for (double* p : fa)
+      if (p) cudaFree(p);
+  }
+  for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
+    LevelF32& G = c->F32[l];
+    float* fa[] = {G.u, G.fu, G.ru, G.uold, G.p, G.w, G.invM, G.K, G.G, G.d, G.Ke, G.Ge};
+    for (float* p : fa)
+      if (p) cudaFree(p);
+  }
+  if (c->g32.valid) cudaGraphExecDestroy(c->g32.exec);
   if (c->ck.stream) cudaStreamSynchronize(c->ck.stream);
   if (c->ck.dev) cudaFree(c->ck.dev);
   if (c->ck.host) cudaFreeHost(c->ck.host);
@@ -1065,6 +1342,21 @@ int hpc_u_entire(hpc_ctx* c, const hpc_mg* mg, double small_k, double Ut, int t,
   return HPC_OK;
 }
 
+int hpc_u_entire_fcg(hpc_ctx* c, const hpc_mg* mg, double small_k, double Ut, int t, double* f_norm,
+                     double mech_tol, int mixed, int* cycles, int* iters) {
+  if (!c || !mg || !f_norm) return arg_fail("bad argument");
+  c->f_norm = *f_norm;
+  int cy = 0;
+  long long it = 0;
+  int rc = u_entire_fcg_dev(c, *mg, small_k, Ut, t, mech_tol, &cy, &it, mixed != 0);
+  if (rc) return rc;
+  if ((rc = hpc_sync(c))) return rc;
+  *f_norm = c->f_norm;
+  if (cycles) *cycles = cy;
+  if (iters) *iters = (int)it;
+  return HPC_OK;
+}
+
 int hpc_phase_field(hpc_ctx* c, const hpc_mg* mg, double lc, int t, double* fd_norm, double pf_tol, int* cycles,
                     int* iters) {
   (void)t;
@@ -1086,7 +1378,15 @@ int hpc_step(hpc_ctx* c, const hpc_step_params* p, double* out) {
   const int L = c->maxlevel;
   int rc, mcy = 0, pcy = 0;
   long long mit = 0, pit = 0;
-  if ((rc = u_entire_dev(c, p->mg_u, p->small_k, U_unit, p->t, p->mech_tol, &mcy, &mit))) return rc;
+  if (p->mech_solver == HPC_MECH_FCG || p->mech_solver == HPC_MECH_MIXED) {
+    if ((rc = u_entire_fcg_dev(c, p->mg_u, p->small_k, U_unit, p->t, p->mech_tol, &mcy, &mit,
+                               p->mech_solver == HPC_MECH_MIXED)))
+      return rc;
+  } else if (p->mech_solver == HPC_MECH_FAS) {
+    if ((rc = u_entire_dev(c, p->mg_u, p->small_k, U_unit, p->t, p->mech_tol, &mcy, &mit))) return rc;
+  } else {
+    return arg_fail("unknown mech_solver");
+  }
   if (p->t == 0) {
     if (p->ut0 <= 0.0) {
       double ue;

@@ -15,8 +15,8 @@ constexpr int kMaxLevels = 16;
 constexpr int kPitchAlign = 4;  // x pitch rounded to 4 doubles (32 B): 16-byte aligned rows
 
 // Geometry of one level as the kernels see it.  Arrays are x-fastest with an x pitch `px` >= nx;
-// padding slots are kept at zero in every vector (and at one in diagonals) so flat vector kernels
-// may run over the padded range.
+// padding slots are kept at zero in every vector and diagonal, so flat vector kernels may run over
+// the padded range.
 struct LevelGeo {
   int nx, ny, nz, px;
   long long plane;  // px * ny
@@ -42,6 +42,14 @@ struct LevelFields {
   uint8_t* bc_host_copy;           // host copies of the axis flags (nx+ny+nz bytes)
 };
 
+// Single-precision mirror of one level for the V-cycle of the precision form (hpc_step with
+// mech_solver HPC_MECH_FCG32): vectors 3n floats, material n floats, allocated on first use.
+struct LevelF32 {
+  float *u, *fu, *ru, *uold, *p, *w, *invM;  // 3n each; invM: inverse diagonal of K
+  float *K, *G, *d;                           // finest level: nodal moduli and phase field
+  float *Ke, *Ge;                             // coarse levels: element moduli
+};
+
 // Device scalar pool layout (doubles).
 enum Scalar : int {
   S_FNORM = 0,    // f_norm of the mechanical solve (pcg_u at t == 0, finest)
@@ -54,10 +62,18 @@ enum Scalar : int {
 };
 constexpr int kMaxRelax = 4096;
 constexpr int S_ZEROS = S_PCG + 3 * (kMaxRelax + 2);  // zero-diagonal counts, one slot per level
-constexpr int kScalarPool = S_ZEROS + 16;
+// flexible-PCG outer solve: per iteration k, delta = (z_k, r_k), gamma = (z_k, r_{k-1}), (p_k, w_k),
+// |r_{k+1}|^2 and (r, M^-1 r) (unused)
+constexpr int S_FCG = S_ZEROS + 16;
+constexpr int kScalarPool = S_FCG + 5 * (kMaxRelax + 2);
 inline int slot_rz(int it) { return S_PCG + 1 + it; }  // it >= -1
 inline int slot_pw(int it) { return S_PCG + (kMaxRelax + 2) + it; }
 inline int slot_rn(int it) { return S_PCG + 2 * (kMaxRelax + 2) + it; }
+inline int slot_fdelta(int k) { return S_FCG + 1 + k; }  // k >= -1
+inline int slot_fgamma(int k) { return S_FCG + (kMaxRelax + 2) + k; }
+inline int slot_fpw(int k) { return S_FCG + 2 * (kMaxRelax + 2) + k; }
+inline int slot_frn(int k) { return S_FCG + 3 * (kMaxRelax + 2) + k; }
+inline int slot_fdummy(int k) { return S_FCG + 4 * (kMaxRelax + 2) + k; }
 
 }  // namespace hpc
 
@@ -67,6 +83,7 @@ struct hpc_ctx {
   double box[6];  // xa xb ya yb za zb
   hpc::LevelGeo L[hpc::kMaxLevels];
   hpc::LevelFields F[hpc::kMaxLevels];
+  hpc::LevelF32 F32[hpc::kMaxLevels];  // precision form (null until first used)
   double* d_old;  // finest d of the previous increment
   cudaStream_t stream;
   int device;
@@ -86,7 +103,7 @@ struct hpc_ctx {
     int valid;
     hpc_mg mg;
     double a, b;  // small_k, Ut (mechanical) or lc (phase field)
-  } gmech, gpf;
+  } gmech, gpf, g32;  // g32: FP32 coarse part of the mixed-precision preconditioner
   int use_graphs;
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
@@ -103,6 +120,11 @@ struct hpc_ctx {
     int t, pending, valid;
     double state[6];
   } ck;
+  // flexible-PCG outer solve of the precision form (hpc_u_entire_fcg): finest-level 3n vectors,
+  // allocated on first use
+  struct Fcg {
+    double *x, *r, *rp, *f, *p;  // iterate, residual, previous residual, right-hand side (fu saved), direction
+  } fcg;
 };
 
 namespace hpc {
@@ -160,6 +182,32 @@ struct MechCall {
 int launch_mech(hpc_ctx* c, const MechCall& m);
 int launch_mech_diag(hpc_ctx* c, int level, bool finest, double small_k, double* out);
 
+// Single-precision operator on the FP32 mirror of a level (EPI_PLAIN, EPI_RESIDUAL, EPI_PCG, EPI_FAS);
+// the residual zeroes Dirichlet rows and sums (r, M^-1 r) into s_out1 and |r|^2 into s_out2 in FP64.
+struct MechCall32 {
+  int level;
+  bool finest;
+  int epi;
+  const float* src;
+  float* out;
+  double small_k;
+  float* fu;          // RESIDUAL: right-hand side
+  const float* invM;  // RESIDUAL: inverse diagonal for (r, M^-1 r)
+  const float* rf;    // FAS: fine residual
+  int fine_level;
+  int s_out0, s_out1, s_out2;
+};
+int launch_mech_f32(hpc_ctx* c, const MechCall32& m);
+// FP32 mirror: u += alpha p, r -= alpha w on F32[level] (Dirichlet rows zero), alpha = scal[s_num]/scal[s_den]
+int launch_mech_update_f32(hpc_ctx* c, int level, int s_num, int s_den, int s_rz_next, int s_rn);
+// FP32 mirror: p = r M^-1 + beta p (beta from scal, 0 if first)
+int launch_dir_update_f32(hpc_ctx* c, int level, bool first, int s_rz, int s_rz_prev);
+int launch_bc_zero_f32(hpc_ctx* c, int level, float* v);  // zero the Dirichlet rows of a 3n vector
+int launch_inject_u_f32(hpc_ctx* c, int lf);             // u_c = u_f(2i), Dirichlet rows 0, uold_c = u_c
+int launch_prolong_f32(hpc_ctx* c, int lf);              // u_f += P(u_c - uold_c), Dirichlet rows 0
+int launch_to_f32(hpc_ctx* c, const double* src, float* dst, long long n);
+int launch_to_f64(hpc_ctx* c, const float* src, double* dst, long long n);
+
 struct PfCall {
   int level;
   int epi;  // EPI_PLAIN, EPI_RESIDUAL, EPI_PCG, EPI_FAS
@@ -182,6 +230,15 @@ int launch_pf_diag(hpc_ctx* c, int level, double lc, double* out);
 // Mechanical CG update: alpha = scal[s_rz]/scal[s_pw]; u += alpha p; r -= alpha w; r = 0 on Dirichlet
 // nodes; scal[s_rz_next] = sum r^2/preM; scal[s_rn] = sum r^2.
 int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
+// Same on explicit arrays: x += alpha p, r -= alpha w (Dirichlet rows zero), alpha = scal[s_num]/scal[s_den].
+int launch_mech_update_on(hpc_ctx* c, int level, double* x, double* r, const double* p, const double* w,
+                          const double* invM, int s_num, int s_den, int s_rz_next, int s_rn);
+// sums (a, b) and (a, c) over a 3n vector of a level into scal[s0], scal[s1] (c may be null)
+int launch_dot2(hpc_ctx* c, int level, const double* a, const double* b, const double* cv, int s0, int s1);
+// flexible direction p = z + beta p, beta = (scal[s_delta] - scal[s_gamma]) / scal[s_delta_prev]
+// (Polak-Ribiere form of flexible CG), beta = 0 if first
+int launch_fcg_dir(hpc_ctx* c, int level, const double* z, double* p, bool first, int s_delta, int s_gamma,
+                   int s_delta_prev);
 int launch_pf_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
 // p = r M^-1 + beta p (beta = scal[s_rz]/scal[s_rz_prev], 0 if first), in place
 int launch_dir_update(hpc_ctx* c, int level, int ncomp, const double* r, const double* invM, double* p, bool first,

@@ -3,6 +3,8 @@
 // deterministic grid reduction of device_common.cuh.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "internal.h"
 
@@ -48,37 +50,123 @@ int row_grid(const LevelGeo& g, int per_sm = 8) {
 // ---------------------------------------------------------------------------------------------
 // PCG updates (mechanical_pcg.cpp:301-321, phase_field_pcg.cpp:192-200)
 // ---------------------------------------------------------------------------------------------
-__global__ void mech_update_kernel(LevelGeo g, double* u, double* r, const double* p, const double* w,
-                                   const double* invM, int s_rz, int s_pw, RedTarget red) {
-  const double alpha = red.scal[s_rz] / red.scal[s_pw];
+// Two x-adjacent slots per thread with 16-byte accesses over the padded layout (the x pitch is a
+// multiple of 4, so a pair never straddles a row; padding slots hold zeros in u, r, p, w and invM
+// and stay zero).  Dirichlet flags exist only on the bottom and top planes.
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+template <typename T>
+__global__ void mech_update_kernel(LevelGeo g, T* u, T* r, const T* p, const T* w, const T* invM, int s_rz, int s_pw,
+                                   RedTarget red) {
+  using V2 = typename Vec2<T>::type;
+  const T alpha = (T)(red.scal[s_rz] / red.scal[s_pw]);
   double rz = 0.0, rn = 0.0;
-  FOR_NODES(g) {
-    const long long n = nidx(g, i, j, kz);
-    const BcFlags bc = bc_flags(g, i, j, kz);
-    const bool fix[3] = {bc.c0, bc.c1, bc.c2};
+  const unsigned half = (unsigned)g.px / 2u, npairs = half * (unsigned)g.ny * (unsigned)g.nz;
+  for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < npairs; q += gridDim.x * blockDim.x) {
+    const unsigned row = q / half;  // j + k * ny
+    const int i = 2 * (int)(q - row * half);
+    const int kz = (int)(row / (unsigned)g.ny), j = (int)(row - (unsigned)kz * (unsigned)g.ny);
+    const long long n = (long long)row * g.px + i;
+    bool fix[2][3] = {{false, false, false}, {false, false, false}};
+    if (g.bz[kz]) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        if (i + h < g.nx) {
+          const BcFlags bc = bc_flags(g, i + h, j, kz);
+          fix[h][0] = bc.c0;
+          fix[h][1] = bc.c1;
+          fix[h][2] = bc.c2;
+        }
+    }
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
       const long long o = n + (long long)m * g.n;
-      u[o] = fma(p[o], alpha, u[o]);
-      double rv = fix[m] ? 0.0 : fma(-w[o], alpha, r[o]);
-      r[o] = rv;
-      rz = fma(rv, rv * invM[o], rz);
-      rn = fma(rv, rv, rn);
+      const V2 pv = *reinterpret_cast<const V2*>(p + o);
+      const V2 wv = *reinterpret_cast<const V2*>(w + o);
+      const V2 mv = *reinterpret_cast<const V2*>(invM + o);
+      V2 uv = *reinterpret_cast<const V2*>(u + o);
+      V2 rv = *reinterpret_cast<const V2*>(r + o);
+      uv.x = fma(pv.x, alpha, uv.x);
+      uv.y = fma(pv.y, alpha, uv.y);
+      rv.x = fix[0][m] ? T(0) : fma(-wv.x, alpha, rv.x);
+      rv.y = fix[1][m] ? T(0) : fma(-wv.y, alpha, rv.y);
+      *reinterpret_cast<V2*>(u + o) = uv;
+      *reinterpret_cast<V2*>(r + o) = rv;
+      rz = fma((double)rv.x, (double)(rv.x * mv.x), rz);
+      rz = fma((double)rv.y, (double)(rv.y * mv.y), rz);
+      rn = fma((double)rv.x, (double)rv.x, rn);
+      rn = fma((double)rv.y, (double)rv.y, rn);
     }
   }
   double v[3] = {rz, rn, 0.0};
   grid_reduce<3>(v, red);
 }
 
-int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn) {
+int launch_mech_update_on(hpc_ctx* c, int level, double* x, double* r, const double* p, const double* w,
+                          const double* invM, int s_num, int s_den, int s_rz_next, int s_rn) {
   const LevelGeo& g = c->L[level];
-  const LevelFields& F = c->F[level];
-  const int grid = row_grid(g);
+  const long long pairs = (long long)(g.px / 2) * g.ny * g.nz;
+  const int grid = (int)std::min<long long>((pairs + kRowThreads - 1) / kRowThreads, (long long)num_sms_v() * 8);
   const int cls = level == c->maxlevel ? HPC_KC_MECH_UPDATE_FINEST : HPC_KC_NONE;
   timing_begin(c, cls);
-  mech_update_kernel<<<grid, kRowThreads, 0, c->stream>>>(g, F.u, F.ru, p, F.w, F.preMu, s_rz, s_pw,
+  mech_update_kernel<<<grid, kRowThreads, 0, c->stream>>>(g, x, r, p, w, invM, s_num, s_den,
                                                           make_red(c, s_rz_next, s_rn, -1));
   timing_end(c, cls);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+
+int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn) {
+  const LevelFields& F = c->F[level];
+  return launch_mech_update_on(c, level, F.u, F.ru, p, F.w, F.preMu, s_rz, s_pw, s_rz_next, s_rn);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Flexible PCG of the precision form: two dot products in one pass, the flexible direction update
+// ---------------------------------------------------------------------------------------------
+__global__ void dot2_kernel(LevelGeo g, const double* a, const double* b, const double* cv, RedTarget red) {
+  double s0 = 0.0, s1 = 0.0;
+  FOR_NODES(g) {
+    const long long n = nidx(g, i, j, kz);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const long long o = n + (long long)m * g.n;
+      const double av = a[o];
+      s0 = fma(av, b[o], s0);
+      if (cv) s1 = fma(av, cv[o], s1);
+    }
+  }
+  double v[2] = {s0, s1};
+  grid_reduce<2>(v, red);
+}
+
+int launch_dot2(hpc_ctx* c, int level, const double* a, const double* b, const double* cv, int s0, int s1) {
+  const LevelGeo& g = c->L[level];
+  dot2_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, a, b, cv, make_red(c, s0, cv ? s1 : -1, -1));
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+
+__global__ void fcg_dir_kernel(LevelGeo g, const double* z, double* p, int first, const double* scal, int s_delta,
+                               int s_gamma, int s_delta_prev) {
+  const double beta = first ? 0.0 : (scal[s_delta] - scal[s_gamma]) / scal[s_delta_prev];
+  FOR_NODES(g) {
+    const long long n = nidx(g, i, j, kz);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const long long o = n + (long long)m * g.n;
+      p[o] = first ? z[o] : fma(beta, p[o], z[o]);
+    }
+  }
+}
+
+int launch_fcg_dir(hpc_ctx* c, int level, const double* z, double* p, bool first, int s_delta, int s_gamma,
+                   int s_delta_prev) {
+  const LevelGeo& g = c->L[level];
+  fcg_dir_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, z, p, first ? 1 : 0, c->scal, s_delta, s_gamma,
+                                                            s_delta_prev);
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
 }
@@ -110,14 +198,15 @@ int launch_pf_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw,
 
 // PCG direction (mechanical_pcg.cpp:274-292, phase_field_pcg.cpp:178-186):
 // z = r M^-1, beta = rz/rz_old (0 on a call's first iteration), p = z + beta p, in place.
-__global__ void dir_update_kernel(LevelGeo g, int ncomp, const double* r, const double* invM, double* p, int first,
+template <typename T>
+__global__ void dir_update_kernel(LevelGeo g, int ncomp, const T* r, const T* invM, T* p, int first,
                                   const double* scal, int s_rz, int s_rz_prev) {
-  const double beta = first ? 0.0 : scal[s_rz] / scal[s_rz_prev];
+  const T beta = first ? T(0) : (T)(scal[s_rz] / scal[s_rz_prev]);
   FOR_NODES(g) {
     const long long n = nidx(g, i, j, kz);
     for (int m = 0; m < ncomp; ++m) {
       const long long o = n + (long long)m * g.n;
-      const double z = r[o] * invM[o];
+      const T z = r[o] * invM[o];
       p[o] = first ? z : fma(beta, p[o], z);
     }
   }
@@ -134,23 +223,24 @@ int launch_dir_update(hpc_ctx* c, int level, int ncomp, const double* r, const d
 // ---------------------------------------------------------------------------------------------
 // Dirichlet conditions (boundary_conditions.cpp:20-154) on the planes that carry any flag
 // ---------------------------------------------------------------------------------------------
-__global__ void bc_kernel(LevelGeo g, double* v, const double* src, int kind, double Ut) {
+template <typename T>
+__global__ void bc_kernel(LevelGeo g, T* v, const T* src, int kind, T Ut) {
   FOR_NODES(g) {
     if (g.bz[kz] == 0) continue;
     const BcFlags bc = bc_flags(g, i, j, kz);
     const long long n = nidx(g, i, j, kz);
     if (kind == 0) {
-      if (bc.c0) v[n] = 0.0;
-      if (bc.c1) v[n + g.n] = 0.0;
-      if (bc.c2) v[n + 2 * g.n] = bc.top ? Ut : 0.0;
+      if (bc.c0) v[n] = T(0);
+      if (bc.c1) v[n + g.n] = T(0);
+      if (bc.c2) v[n + 2 * g.n] = bc.top ? Ut : T(0);
     } else if (kind == 1) {
       if (bc.c0) v[n] = src[n];
       if (bc.c1) v[n + g.n] = src[n + g.n];
       if (bc.c2) v[n + 2 * g.n] = src[n + 2 * g.n];
     } else {
-      if (bc.c0) v[n] = 0.0;
-      if (bc.c1) v[n + g.n] = 0.0;
-      if (bc.c2) v[n + 2 * g.n] = 0.0;
+      if (bc.c0) v[n] = T(0);
+      if (bc.c1) v[n + g.n] = T(0);
+      if (bc.c2) v[n + 2 * g.n] = T(0);
     }
   }
 }
@@ -241,15 +331,16 @@ int launch_inject(hpc_ctx* c, int lf, const double* f, double* co, int ncomp) {
 }
 
 // coarsen_u (:106-121): inject, Dirichlet_BD on the coarse level, save uold.
-__global__ void inject_u_kernel(LevelGeo gc, LevelGeo gf, const double* uf, double* uc, double* uold, double Ut) {
+template <typename T>
+__global__ void inject_u_kernel(LevelGeo gc, LevelGeo gf, const T* uf, T* uc, T* uold, T Ut) {
   FOR_NODES(gc) {
     const long long nc = nidx(gc, i, j, kz), nf = nidx(gf, 2 * i, 2 * j, 2 * kz);
-    double v[3] = {uf[nf], uf[nf + gf.n], uf[nf + 2 * gf.n]};
+    T v[3] = {uf[nf], uf[nf + gf.n], uf[nf + 2 * gf.n]};
     if (gc.bz[kz]) {
       const BcFlags bc = bc_flags(gc, i, j, kz);
-      if (bc.c0) v[0] = 0.0;
-      if (bc.c1) v[1] = 0.0;
-      if (bc.c2) v[2] = bc.top ? Ut : 0.0;
+      if (bc.c0) v[0] = T(0);
+      if (bc.c1) v[1] = T(0);
+      if (bc.c2) v[2] = bc.top ? Ut : T(0);
     }
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
@@ -297,8 +388,9 @@ int launch_restrict(hpc_ctx* c, int lf, const double* rf, const double* Fic, dou
 
 // refine_standard_routine (:416-520) as a gather over fine nodes, with the reference's term order;
 // optionally followed by Dirichlet_BD on the fine level (refine_u, :536-549).
-__global__ void prolong_kernel(LevelGeo gc, LevelGeo gf, const double* uc, const double* ucold, double* uf, int ncomp,
-                               int apply_bc, double Ut) {
+template <typename T>
+__global__ void prolong_kernel(LevelGeo gc, LevelGeo gf, const T* uc, const T* ucold, T* uf, int ncomp, int apply_bc,
+                               T Ut) {
   FOR_NODES(gf) {
     const int ox = i & 1, oy = j & 1, oz = kz & 1;
     const int ic = (i + 1) >> 1, jc = (j + 1) >> 1, kc = (kz + 1) >> 1;
@@ -306,31 +398,31 @@ __global__ void prolong_kernel(LevelGeo gc, LevelGeo gf, const double* uc, const
     BcFlags bc{false, false, false, false};
     if (apply_bc && gf.bz[kz]) bc = bc_flags(gf, i, j, kz);
     for (int m = 0; m < ncomp; ++m) {
-      const double* a = uc + m * gc.n;
-      const double* o = ucold + m * gc.n;
-      auto E = [&](int x, int y, int z) -> double {
+      const T* a = uc + m * gc.n;
+      const T* o = ucold + m * gc.n;
+      auto E = [&](int x, int y, int z) -> T {
         const long long q = nidx(gc, x, y, z);
         return a[q] - o[q];
       };
-      double add;
+      T add;
       if (!ox && !oy && !oz) add = E(ic, jc, kc);
-      else if (ox && !oy && !oz) add = 0.5 * (E(ic, jc, kc) + E(ic - 1, jc, kc));
-      else if (!ox && oy && !oz) add = 0.5 * (E(ic, jc, kc) + E(ic, jc - 1, kc));
-      else if (!ox && !oy && oz) add = 0.5 * (E(ic, jc, kc) + E(ic, jc, kc - 1));
+      else if (ox && !oy && !oz) add = T(0.5) * (E(ic, jc, kc) + E(ic - 1, jc, kc));
+      else if (!ox && oy && !oz) add = T(0.5) * (E(ic, jc, kc) + E(ic, jc - 1, kc));
+      else if (!ox && !oy && oz) add = T(0.5) * (E(ic, jc, kc) + E(ic, jc, kc - 1));
       else if (ox && oy && !oz)
-        add = 0.25 * (E(ic, jc, kc) + E(ic, jc - 1, kc) + E(ic - 1, jc, kc) + E(ic - 1, jc - 1, kc));
+        add = T(0.25) * (E(ic, jc, kc) + E(ic, jc - 1, kc) + E(ic - 1, jc, kc) + E(ic - 1, jc - 1, kc));
       else if (ox && !oy && oz)
-        add = 0.25 * (E(ic, jc, kc) + E(ic - 1, jc, kc - 1) + E(ic, jc, kc - 1) + E(ic - 1, jc, kc));
+        add = T(0.25) * (E(ic, jc, kc) + E(ic - 1, jc, kc - 1) + E(ic, jc, kc - 1) + E(ic - 1, jc, kc));
       else if (!ox && oy && oz)
-        add = 0.25 * (E(ic, jc, kc) + E(ic, jc - 1, kc - 1) + E(ic, jc, kc - 1) + E(ic, jc - 1, kc));
+        add = T(0.25) * (E(ic, jc, kc) + E(ic, jc - 1, kc - 1) + E(ic, jc, kc - 1) + E(ic, jc - 1, kc));
       else
-        add = 0.125 * (E(ic, jc, kc) + E(ic, jc - 1, kc) + E(ic - 1, jc, kc) + E(ic - 1, jc - 1, kc) +
-                       E(ic, jc, kc - 1) + E(ic - 1, jc, kc - 1) + E(ic, jc - 1, kc - 1) + E(ic - 1, jc - 1, kc - 1));
-      double v = uf[nf + m * gf.n] + add;
+        add = T(0.125) * (E(ic, jc, kc) + E(ic, jc - 1, kc) + E(ic - 1, jc, kc) + E(ic - 1, jc - 1, kc) +
+                          E(ic, jc, kc - 1) + E(ic - 1, jc, kc - 1) + E(ic, jc - 1, kc - 1) + E(ic - 1, jc - 1, kc - 1));
+      T v = uf[nf + m * gf.n] + add;
       if (apply_bc) {
-        if (m == 0 && bc.c0) v = 0.0;
-        if (m == 1 && bc.c1) v = 0.0;
-        if (m == 2 && bc.c2) v = bc.top ? Ut : 0.0;
+        if (m == 0 && bc.c0) v = T(0);
+        if (m == 1 && bc.c1) v = T(0);
+        if (m == 2 && bc.c2) v = bc.top ? Ut : T(0);
       }
       uf[nf + m * gf.n] = v;
     }
@@ -385,7 +477,7 @@ __global__ void choice_kernel(ChoiceK a) {
         for (int m = 0; m < 3; ++m) {
           double un[8];
           load8(a.u + m * g.n, g, i, j, k, un);
-          sf_forward(un, s, gx[m], gy[m], gz[m], nullptr);
+          sf_forward(un, s, gx[m], gy[m], gz[m], (double*)nullptr);
         }
         double tr = 0.0, pp = 0.0, pn = 0.0;
 #pragma unroll
@@ -520,7 +612,7 @@ __global__ void strain_history_kernel(LevelGeo g, const double* u, const double*
       for (int m = 0; m < 3; ++m) {
         double un[8];
         load8(u + m * g.n, g, i, j, k, un);
-        sf_forward(un, s, gx[m], gy[m], gz[m], nullptr);
+        sf_forward(un, s, gx[m], gy[m], gz[m], (double*)nullptr);
       }
       double tmp = 0.0;
 #pragma unroll
@@ -628,7 +720,7 @@ __global__ void ue_kernel(LevelGeo g, const double* u, const double* bulK, const
       for (int m = 0; m < 3; ++m) {
         double un[8];
         load8(u + m * g.n, g, i, j, k, un);
-        sf_forward(un, s, gx[m], gy[m], gz[m], nullptr);
+        sf_forward(un, s, gx[m], gy[m], gz[m], (double*)nullptr);
       }
 #pragma unroll
       for (int gp = 0; gp < 8; ++gp) {
@@ -761,4 +853,70 @@ int launch_zero_count(hpc_ctx* c, int level, int ncomp, const double* v, int slo
   return HPC_OK;
 }
 
+}  // namespace hpc
+
+// ---------------------------------------------------------------------------------------------
+// Precision form: the V-cycle's vector kernels on the FP32 mirror of the levels (homogeneous
+// Dirichlet values: the cycle solves for a correction), and FP64 <-> FP32 conversions.
+// ---------------------------------------------------------------------------------------------
+namespace hpc {
+namespace {
+template <typename S, typename D>
+__global__ void convert_kernel(const S* src, D* dst, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    dst[q] = (D)src[q];
+}
+int flat_grid(long long n) {
+  const long long blocks = (n + kRowThreads - 1) / kRowThreads, cap = (long long)num_sms_v() * 8;
+  return (int)(blocks < cap ? blocks : cap);
+}
+}  // namespace
+
+int launch_to_f32(hpc_ctx* c, const double* src, float* dst, long long n) {
+  convert_kernel<<<flat_grid(n), kRowThreads, 0, c->stream>>>(src, dst, n);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+int launch_to_f64(hpc_ctx* c, const float* src, double* dst, long long n) {
+  convert_kernel<<<flat_grid(n), kRowThreads, 0, c->stream>>>(src, dst, n);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+
+int launch_mech_update_f32(hpc_ctx* c, int level, int s_num, int s_den, int s_rz_next, int s_rn) {
+  const LevelGeo& g = c->L[level];
+  const LevelF32& F = c->F32[level];
+  const long long pairs = (long long)(g.px / 2) * g.ny * g.nz;
+  const int grid = (int)std::min<long long>((pairs + kRowThreads - 1) / kRowThreads, (long long)num_sms_v() * 8);
+  mech_update_kernel<float><<<grid, kRowThreads, 0, c->stream>>>(g, F.u, F.ru, F.p, F.w, F.invM, s_num, s_den,
+                                                                  make_red(c, s_rz_next, s_rn, -1));
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+int launch_dir_update_f32(hpc_ctx* c, int level, bool first, int s_rz, int s_rz_prev) {
+  const LevelGeo& g = c->L[level];
+  const LevelF32& F = c->F32[level];
+  dir_update_kernel<float><<<row_grid(g), kRowThreads, 0, c->stream>>>(g, 3, F.ru, F.invM, F.p, first ? 1 : 0,
+                                                                       c->scal, s_rz, s_rz_prev);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+int launch_bc_zero_f32(hpc_ctx* c, int level, float* v) {
+  const LevelGeo& g = c->L[level];
+  bc_kernel<float><<<row_grid(g), kRowThreads, 0, c->stream>>>(g, v, nullptr, 2, 0.0f);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+int launch_inject_u_f32(hpc_ctx* c, int lf) {
+  inject_u_kernel<float><<<row_grid(c->L[lf - 1]), kRowThreads, 0, c->stream>>>(
+      c->L[lf - 1], c->L[lf], c->F32[lf].u, c->F32[lf - 1].u, c->F32[lf - 1].uold, 0.0f);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+int launch_prolong_f32(hpc_ctx* c, int lf) {
+  prolong_kernel<float><<<row_grid(c->L[lf]), kRowThreads, 0, c->stream>>>(
+      c->L[lf - 1], c->L[lf], c->F32[lf - 1].u, c->F32[lf - 1].uold, c->F32[lf].u, 3, 1, 0.0f);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
 }  // namespace hpc

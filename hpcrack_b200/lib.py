@@ -39,7 +39,7 @@ class hpc_mg(C.Structure):
 class hpc_step_params(C.Structure):
     _fields_ = [("t", C.c_int), ("mg_u", hpc_mg), ("mg_d", hpc_mg), ("small_k", C.c_double), ("lc", C.c_double),
                 ("voxel_size", C.c_double), ("ut0", C.c_double), ("du", C.c_double), ("du_factor", C.c_double),
-                ("mech_tol", C.c_double), ("pf_tol", C.c_double)]
+                ("mech_tol", C.c_double), ("pf_tol", C.c_double), ("mech_solver", C.c_int)]
 
 
 _vp = C.c_void_p
@@ -84,6 +84,7 @@ SIGNATURES = {
     "hpc_u_entire": [_ctx, C.POINTER(hpc_mg), _d, _d, _i, _dp, _d, _ip, _ip],
     "hpc_phase_field": [_ctx, C.POINTER(hpc_mg), _d, _i, _dp, _d, _ip, _ip],
     "hpc_step": [_ctx, C.POINTER(hpc_step_params), _dp],
+    "hpc_u_entire_fcg": [_ctx, C.POINTER(hpc_mg), _d, _d, _i, _dp, _d, _i, _ip, _ip],
     "hpc_mp_choice": [_ctx],
     "hpc_mp_all_element": [_ctx, _d],
     "hpc_vr_all_level": [_ctx, _i],

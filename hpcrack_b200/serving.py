@@ -71,8 +71,9 @@ def default_footprint(w: ms.Workload) -> int:
     return Hierarchy.footprint(w.maxlevel, w.element_nb, x0=w.x_start)
 
 
-def run_request(solver, w: ms.Workload, increments: int):
-    """One fracture run on an allocated solver: material from the image, pre-crack, increments."""
+def run_request(solver, w: ms.Workload, increments: int, mech_solver: int = 0):
+    """One fracture run on an allocated solver: material from the image, pre-crack, increments
+    (mech_solver 0: the reference's FAS cycles, 1: flexible PCG preconditioned by one V-cycle)."""
     nx, ny, nz = w.nodes
     solver.image_material(w.image, (nx, ny, nz), w.table(), w.voxel_size)
     if w.crack:
@@ -83,18 +84,20 @@ def run_request(solver, w: ms.Workload, increments: int):
     outs = []
     for t in range(increments):
         outs.append(solver.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
-                                dU_factor=w.du_factor, mech_tol=w.mech_tol, pf_tol=w.pf_tol))
+                                dU_factor=w.du_factor, mech_tol=w.mech_tol, pf_tol=w.pf_tol,
+                                mech_solver=mech_solver))
     return outs
 
 
 class SolveServer:
     def __init__(self, hbm_budget: int, slots: int, solver_factory: Callable = None,
-                 footprint: Callable = None, keep_fields: bool = False):
+                 footprint: Callable = None, keep_fields: bool = False, mech_solver: int = 0):
         self.budget = int(hbm_budget)
         self.slots = int(slots)
         self.factory = solver_factory or default_factory()
         self.footprint = footprint or default_footprint
         self.keep_fields = keep_fields
+        self.mech_solver = int(mech_solver)
         self._cv = threading.Condition()
         self._pending: list[Request] = []
         self._closed = False
@@ -184,7 +187,7 @@ class SolveServer:
             solver = None
             try:
                 solver = self.factory(req.workload)
-                outs = run_request(solver, req.workload, req.increments)
+                outs = run_request(solver, req.workload, req.increments, self.mech_solver)
                 fields = None
                 if self.keep_fields:
                     L = req.workload.maxlevel

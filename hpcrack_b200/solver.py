@@ -21,6 +21,7 @@ BULK, G, GC, D, H, FD, KE, GE, R, DOLD, DOLDF = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10
 U, FU, RU, UOLD = 16, 17, 18, 19
 VECTOR_FIELDS = (U, FU, RU, UOLD)
 KC_MECH_PCG_FINEST, KC_PF_PCG_FINEST, KC_MECH_UPDATE_FINEST = 0, 1, 2
+MECH_FAS, MECH_FCG, MECH_MIXED = 0, 1, 2  # hpc_step_params.mech_solver
 
 
 def _dptr(a: np.ndarray):
@@ -228,6 +229,16 @@ class Hierarchy:
         self._c("hpc_u_entire", C.byref(mg), small_k, Ut, t, C.byref(fn), mech_tol, C.byref(cy), C.byref(it))
         return cy.value, it.value, fn.value
 
+    def u_entire_fcg(self, mg5, small_k, Ut, t, f_norm, mech_tol=1e-6, mixed=False):
+        """Flexible PCG with one V-cycle per iteration as the preconditioner (FP32 cycle if mixed)."""
+        mg = mg_params(mg5)
+        fn = C.c_double(f_norm)
+        cy = C.c_int(0)
+        it = C.c_int(0)
+        self._c("hpc_u_entire_fcg", C.byref(mg), small_k, Ut, t, C.byref(fn), mech_tol, int(bool(mixed)),
+                C.byref(cy), C.byref(it))
+        return cy.value, it.value, fn.value
+
     def phase_field(self, mg5, lc, t, fd_norm, pf_tol=1e-12):
         fn = C.c_double(fd_norm)
         cy, it = C.c_int(0), C.c_int(0)
@@ -236,9 +247,11 @@ class Hierarchy:
         return cy.value, it.value, fn.value
 
     def step(self, t, mg_u, mg_d, small_k, lc, voxel_size, ut0=0.0, dU=0.0, dU_factor=1.5e-3, mech_tol=1e-6,
-             pf_tol=1e-12):
+             pf_tol=1e-12, mech_solver=MECH_FAS):
+        """One staggered increment; mech_solver MECH_FAS (the reference's V-cycles), MECH_FCG (flexible
+        PCG preconditioned by one V-cycle per iteration) or MECH_MIXED (the same with the V-cycle in FP32)."""
         p = _L.hpc_step_params(int(t), mg_params(mg_u), mg_params(mg_d), small_k, lc, voxel_size, ut0, dU, dU_factor,
-                               mech_tol, pf_tol)
+                               mech_tol, pf_tol, int(mech_solver))
         out = (C.c_double * 8)()
         self._c("hpc_step", C.byref(p), out)
         return list(out)

@@ -92,7 +92,13 @@ typedef struct {
   double du_factor;    /* 1.5e-3 in the reference (crack_propagation.cpp:76) */
   double mech_tol;     /* squared ratio |r|^2/|f|^2 (1e-6 in mechanical_displacement.cpp:88) */
   double pf_tol;       /* squared tests of phase_field.cpp:30-43 (1e-12 there) */
+  int mech_solver;     /* HPC_MECH_FAS (0): the reference's FAS V-cycles (plain form);
+                          HPC_MECH_FCG (1): flexible PCG preconditioned by one FP64 V-cycle;
+                          HPC_MECH_MIXED (2): the precision form, the same with the V-cycle in FP32
+                          (coarsest solve FP64); see hpc_u_entire_fcg */
 } hpc_step_params;
+
+enum { HPC_MECH_FAS = 0, HPC_MECH_FCG = 1, HPC_MECH_MIXED = 2 };
 
 /* ---------------- context ---------------- */
 
@@ -115,8 +121,8 @@ void* hpc_stream(hpc_ctx* ctx);
 /* Kernel classes that can be timed with CUDA events on the context's stream. */
 enum hpc_kernel_class {
   HPC_KC_NONE = -1,
-  HPC_KC_MECH_PCG_FINEST = 0,   /* fused direction update + K(d) p + (p, w) on the finest level */
-  HPC_KC_PF_PCG_FINEST = 1,     /* fused direction update + A_d p + (p, w) on the finest level */
+  HPC_KC_MECH_PCG_FINEST = 0,   /* w = K(d) p and (p, w) on the finest level (FP64) */
+  HPC_KC_PF_PCG_FINEST = 1,     /* w = A_d p and (p, w) on the finest level */
   HPC_KC_MECH_UPDATE_FINEST = 2 /* u += alpha p, r -= alpha w, rz and |r|^2 on the finest level */
 };
 /* Records a start/stop event pair around every launch of `kernel_class` from now on (HPC_KC_NONE
@@ -180,6 +186,14 @@ int hpc_u_entire(hpc_ctx* ctx, const hpc_mg* mg, double small_k, double Ut, int 
 /* phase_field (phase_field.cpp:15-57). */
 int hpc_phase_field(hpc_ctx* ctx, const hpc_mg* mg, double lc, int t, double* fd_norm, double pf_tol,
                     int* cycles, int* iters);
+/* No counterpart in the reference: the mechanical solve of u_entire (mechanical_displacement.cpp:25-115)
+ * by flexible PCG on the finest level (true residual, dot products and updates in FP64),
+ * preconditioned by one V-cycle of cycle_u's kind per iteration, in FP64 (mixed = 0) or on
+ * single-precision copies of the levels with an FP64 coarsest solve (mixed = 1, the precision form);
+ * same stopping test |r|^2/|f|^2 <= mech_tol, f_norm from the reactions at t == 0, reactions into
+ * fu at the end.  *cycles = outer iterations (= V-cycles), *iters = finest smoother iterations. */
+int hpc_u_entire_fcg(hpc_ctx* ctx, const hpc_mg* mg, double small_k, double Ut, int t, double* f_norm,
+                     double mech_tol, int mixed, int* cycles, int* iters);
 /* One staggered increment (crack_propagation.cpp:65-121).  out[8] = {Ut, F (u_proportion*FeW),
  * delta_d_max, d_max, mech cycles, pf cycles, mech finest iters, pf finest iters}. */
 int hpc_step(hpc_ctx* ctx, const hpc_step_params* p, double* out);

@@ -43,5 +43,6 @@ def test_admission_under_tight_budget():
     need = max(sv.default_footprint(r.workload) for r in reqs)
     srv = sv.SolveServer(hbm_budget=need, slots=3)
     res = srv.replay(reqs)
-    assert srv.peak_active == 1 and srv.peak_used <= need
+    # never more than the budget in use; the three together do not fit, the two smaller ones may
+    assert srv.peak_used <= need and srv.peak_active <= 2
     assert all(len(r.outputs) == 3 for r in res)
