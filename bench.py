@@ -69,6 +69,8 @@ def parse_args():
     ap.add_argument("--compare-forms", action="store_true",
                     help="run --steps increments with the plain form and with --mech-solver (default mixed) and "
                          "report solves/s of both and the per-field error against the plain run")
+    ap.add_argument("--mg-u", default="", metavar="NU0,NU1,NU2,GAMMA",
+                    help="override the workload's mechanical multigrid parameters (ncy stays)")
     ap.add_argument("--requests", type=int, default=24, help="requests in a --serve sample")
     ap.add_argument("--increments", type=int, default=0, help="increments per request (default 10 serve, 5 batch)")
     ap.add_argument("--slots", type=int, default=8, help="concurrent requests on the GPU")
@@ -97,6 +99,10 @@ def run_serving(args, local):
         reqs = sv.serve_mix(args.requests, args.serve, seed=7, increments=inc, **kw)
         metric, form = "solves/s", f"served: {args.requests} requests, Poisson arrivals at {args.serve}/s (seed 7), " \
                                    f"{inc} increments each"
+    if args.mg_u:
+        v = tuple(int(x) for x in args.mg_u.split(","))
+        for q in reqs:
+            q.workload.mg_u = v + (q.workload.mg_u[4],)
     srv = sv.SolveServer(budget, args.slots, solver_factory=sv.default_factory(local),
                          mech_solver=MECH_SOLVERS[args.mech_solver])
     t0 = time.perf_counter()
@@ -110,17 +116,27 @@ def run_serving(args, local):
     line = {"metric": metric, "value": st["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
             "dtype": "f64", "data": "synthetic", "config": {"workload": form, "slots": args.slots,
                                                             "hbm_budget_gb": args.hbm_budget_gb,
-                                                            "mech_solver": args.mech_solver},
+                                                            "mech_solver": args.mech_solver,
+                                                            "mg_u": list(reqs[0].workload.mg_u)},
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "wall_s": wall,
             "mdof_iter_per_s": dof_iters / wall / 1e6, "peak_active": srv.peak_active,
             "peak_hbm_gb": srv.peak_used / (1 << 30)}
     print(json.dumps(line), flush=True)
 
 
+def workload(args):
+    from hpcrack_b200 import microstructure as ms
+    w = ms.make_workload(args.workload)
+    if args.mg_u:
+        v = tuple(int(x) for x in args.mg_u.split(","))
+        w.mg_u = v + (w.mg_u[4],)
+    return w
+
+
 def run_kernel_only(args, local):
     """A short, bounded program for profilers: material setup, then pcg_u(NB) on the finest level."""
     from hpcrack_b200 import microstructure as ms
-    w = ms.make_workload(args.workload)
+    w = workload(args)
     hier = load_specimen(w, local)
     hier.mp_choice()
     hier.mp_all_element(w.small_k)
@@ -133,7 +149,7 @@ def run_kernel_only(args, local):
 def run_profile_cycles(args, local):
     """A short, bounded program for profilers: two increments whose V-cycle counts are capped at K."""
     from hpcrack_b200 import microstructure as ms
-    w = ms.make_workload(args.workload)
+    w = workload(args)
     hier = load_specimen(w, local)
     K = args.profile_cycles
     mg_u = tuple(w.mg_u[:4]) + (K,)
@@ -273,7 +289,7 @@ def run_reference(args, rank, world):
     from hpcrack_b200 import microstructure as ms
     if rank != 0:
         return
-    w = ms.make_workload(args.workload)
+    w = workload(args)
     vals = []
     for _ in range(max(args.warmup, 0)):
         cpu_reference_sample(w)
@@ -338,7 +354,7 @@ def run_b200(args, rank, world, local):
     from hpcrack_b200.solver import KC_MECH_PCG_FINEST, U, D, H, FU, DOLDF
 
     torch.cuda.set_device(local)
-    w = ms.make_workload(args.workload)
+    w = workload(args)
     nx, ny, nz = w.nodes
     N = nx * ny * nz
     hier = load_specimen(w, local)
@@ -471,7 +487,7 @@ def run_compare_forms(args, local):
     from hpcrack_b200 import microstructure as ms
     from hpcrack_b200.solver import U, D, H
     torch.cuda.set_device(local)
-    w = ms.make_workload(args.workload)
+    w = workload(args)
     res = {}
     for name in ("fas", args.mech_solver if args.mech_solver != "fas" else "mixed"):
         hier = load_specimen(w, local)
