@@ -35,6 +35,7 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 PCG_APPLY_BYTES_PER_NODE = 73
 MECH_SOLVERS = {"fas": 0, "fcg": 1, "mixed": 2}
+
 # DRAM bytes (read + write) per launch of the finest PCG apply: the ncu capture of
 # profiles/mech_pcg_apply_mid193.md measured 440.5 MB + 153.1 MB on the 193^3 level (7,189,057 nodes,
 # 82.6 B/node); other sizes scale that per-node figure by their node count (traffic grows with the
@@ -55,6 +56,11 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-timing", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="measure the element kernels' strip shapes on first use (hpc_set_autotune) instead of "
+                         "the latency model's choice")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the precision-form measurement on the same increments")
     ap.add_argument("--kernel-only", type=int, default=0, metavar="NB",
                     help="profiling driver: set the specimen up, run one finest-level pcg_u with NB iterations "
                          "(NB launches of the dominant kernel) and exit")
@@ -104,7 +110,11 @@ def run_serving(args, local):
         for q in reqs:
             q.workload.mg_u = v + (q.workload.mg_u[4],)
     srv = sv.SolveServer(budget, args.slots, solver_factory=sv.default_factory(local),
-                         mech_solver=MECH_SOLVERS[args.mech_solver])
+                         mech_solver=MECH_SOLVERS[args.mech_solver], precision_mg=not args.mg_u)
+    from hpcrack_b200.solver import PRECISION_MG
+    mg_used = reqs[0].workload.mg_u
+    if args.mech_solver != "fas" and not args.mg_u:
+        mg_used = tuple(PRECISION_MG) + (mg_used[4],)
     t0 = time.perf_counter()
     res = srv.replay(reqs)
     wall = time.perf_counter() - t0
@@ -117,7 +127,7 @@ def run_serving(args, local):
             "dtype": "f64", "data": "synthetic", "config": {"workload": form, "slots": args.slots,
                                                             "hbm_budget_gb": args.hbm_budget_gb,
                                                             "mech_solver": args.mech_solver,
-                                                            "mg_u": list(reqs[0].workload.mg_u)},
+                                                            "mg_u": list(mg_used)},
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "wall_s": wall,
             "mdof_iter_per_s": dof_iters / wall / 1e6, "peak_active": srv.peak_active,
             "peak_hbm_gb": srv.peak_used / (1 << 30)}
@@ -351,13 +361,15 @@ def run_b200(args, rank, world, local):
     import torch
     from hpcrack_b200 import microstructure as ms
     from hpcrack_b200 import replicas
-    from hpcrack_b200.solver import KC_MECH_PCG_FINEST, U, D, H, FU, DOLDF
+    from hpcrack_b200.solver import KC_MECH_PCG_FINEST, U, D, H, FU, DOLDF, Hierarchy
 
     torch.cuda.set_device(local)
     w = workload(args)
     nx, ny, nz = w.nodes
     N = nx * ny * nz
     hier = load_specimen(w, local)
+    if args.autotune:
+        hier.set_autotune(True)
     stream = torch.cuda.ExternalStream(hier.stream())
 
     solver = MECH_SOLVERS[args.mech_solver]
@@ -393,6 +405,7 @@ def run_b200(args, rank, world, local):
     clocks = sampler.stop()
     launches = hier.launch_count() - launches0
     ms_total = e0.elapsed_time(e1)
+    u_plain_final = hier.get(U, w.maxlevel) if (not args.no_forms and args.mech_solver == "fas") else None
     kn, kms = hier.kernel_time() if not args.no_kernel_timing else (0, 0.0)
     hier.kernel_timing(-1)
 
@@ -465,12 +478,53 @@ def run_b200(args, rank, world, local):
                    "sample": f"failed: {exc}"}
 
     hier.close()
+
+    # ------------------------------------------------------------ the precision form on the same increments
+    forms = None
+    if not args.no_forms and args.mech_solver == "fas":
+        wp = workload(args)
+        from hpcrack_b200.solver import PRECISION_MG
+        wp.mg_u = tuple(PRECISION_MG) + (wp.mg_u[4],)
+        hp = load_specimen(wp, local)
+        sp = torch.cuda.ExternalStream(hp.stream())
+
+        def pstep(tt):
+            return hp.step(tt, wp.mg_u, wp.mg_d, wp.small_k, wp.lc, wp.voxel_size, ut0=wp.ut0, dU=wp.du,
+                           dU_factor=wp.du_factor, mech_tol=wp.mech_tol, pf_tol=wp.pf_tol,
+                           mech_solver=MECH_SOLVERS["mixed"])
+        for tt in range(args.warmup):
+            pstep(tt)
+        barrier(world)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(sp)
+        pouts = [pstep(args.warmup + i) for i in range(args.steps)]
+        g1.record(sp)
+        torch.cuda.synchronize()
+        barrier(world)
+        p_ms, _ = replicas.aggregate(g0.elapsed_time(g1), 0.0, world)
+        u_mixed = hp.get(U, wp.maxlevel)
+        hp.close()
+        forms = {"plain": {"solves_per_s": world * args.steps / (max_ms / 1e3),
+                           "v_cycles": [int(o[4]) for o in outs]},
+                 "mixed": {"solves_per_s": world * args.steps / (p_ms / 1e3), "ms_per_step": p_ms / args.steps,
+                           "v_cycles": [int(o[4]) for o in pouts], "mg_u": list(wp.mg_u),
+                           "what": "flexible PCG in FP64 (true residual, dots, updates) preconditioned by one "
+                                   "FP32 V-cycle per iteration (FP64 coarsest solve); same increments, same "
+                                   "FP64 stopping test |r|/|f| <= 1e-8"},
+                 "speedup_mixed_vs_plain": max_ms / p_ms}
+        if u_plain_final is not None:
+            import numpy as np
+            forms["mixed"]["u_rel_l2_vs_plain"] = float(np.linalg.norm(u_mixed - u_plain_final) /
+                                                        np.linalg.norm(u_plain_final))
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": workload_config(w, world, args.mech_solver), "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cpu,
+                "roofline": roofline, "cpu_baseline": cpu, "forms": forms,
+                "strip_shapes": ({"autotuned": [list(x) for x in Hierarchy.tuned_shapes()]} if args.autotune
+                                 else "latency model (choose_strips)"),
                 "solves_per_s": world * args.steps / (max_ms / 1e3),
                 "steps_detail": [{"t": t_first + i, "mech_cycles": int(o[4]), "pf_cycles": int(o[5]),
                                   "mech_iters": int(o[6]), "pf_iters": int(o[7]), "F": o[1], "dmax": o[3]}

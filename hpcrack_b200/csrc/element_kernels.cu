@@ -225,6 +225,16 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
         continue;
       }
       const int rr = r - 1, ey = y0 - 1 + rr;
+      if (EPI == EPI_RESIDUAL && rr >= 1 && kk >= z0 && lane >= 1 && lane <= 30 && x < k.g.nx && ey < k.g.ny) {
+        // the epilogue reads f and M^-1 of this row's output node: start them towards L2 now, so
+        // their latency overlaps the element math instead of following it
+        const long long n = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(k.fu + n + m * k.g.n));
+          if (k.invM) asm volatile("prefetch.global.L2 [%0];" ::"l"(k.invM + n + m * k.g.n));
+        }
+      }
       // ---- element (x, ey, kk) from stream rows si-1 (y = ey) and si (y = ey+1)
       T f[3][8];
       const bool valid = lane < 31 && x >= 0 && x <= k.g.nx - 2 && ey >= 0 && ey <= k.g.ny - 2 && kk >= 0 &&
@@ -403,18 +413,98 @@ static int kernel_cfg(Kern kern, size_t smem, int* per_sm_out) {
   return HPC_OK;
 }
 
-// Launches a strip kernel with the occupancy the device allows (persistent grid), choosing the
-// strip shape of the level from the number of resident warp slots.
+// Strip shapes chosen by measurement (hpc_set_autotune), per kernel, device and level size; shared
+// by every context of the process once measured.
+struct TunedShape {
+  const void* fn;
+  int device, nx, ny, nz, wy, cz;
+};
+static std::mutex g_tune_mu;
+static TunedShape g_tuned[512];
+static int g_ntuned = 0;
+
+static bool tuned_shape(const void* fn, int dev, const LevelGeo& g, StripGeo* out) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  for (int i = 0; i < g_ntuned; ++i) {
+    const TunedShape& t = g_tuned[i];
+    if (t.fn == fn && t.device == dev && t.nx == g.nx && t.ny == g.ny && t.nz == g.nz) {
+      *out = strip_geo(g, t.wy, t.cz);
+      return true;
+    }
+  }
+  return false;
+}
+
+static int grid_for(const StripGeo& sg, long long cap) {
+  const long long need = (sg.nstrips + kWarps - 1) / kWarps;
+  return (int)(need < cap ? need : cap);
+}
+
+// Times every candidate shape on the live arguments (element kernels are pure functions of their
+// inputs: a repeated launch rewrites the same outputs and reductions) and keeps the fastest.
+template <class Kern, class Args>
+static int autotune_shape(hpc_ctx* c, Kern kern, Args a, size_t smem, long long cap, StripGeo* best) {
+  static const int wys[] = {8, 4, 2};
+  static const int czs[] = {32, 16, 8, 4, 2};
+  cudaEvent_t e0, e1;
+  HPC_CUDA(cudaEventCreate(&e0));
+  HPC_CUDA(cudaEventCreate(&e1));
+  float best_ms = 1e30f;
+  *best = choose_strips(a.g, (long long)num_sms() * 4);
+  int rc = HPC_OK;
+  for (int wy : wys)
+    for (int cz : czs) {
+      a.sg = strip_geo(a.g, wy, cz);
+      const int grid = grid_for(a.sg, cap);
+      if (grid <= 0 || (size_t)grid * 3 > c->partials_cap) continue;
+      kern<<<grid, kWarps * 32, smem, c->stream>>>(a);
+      cudaEventRecord(e0, c->stream);
+      kern<<<grid, kWarps * 32, smem, c->stream>>>(a);
+      kern<<<grid, kWarps * 32, smem, c->stream>>>(a);
+      cudaEventRecord(e1, c->stream);
+      c->launches += 3;
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e == cudaSuccess) e = cudaGetLastError();
+      if (e != cudaSuccess) {
+        rc = cuda_fail(e, "autotune launch");
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) {
+        best_ms = ms;
+        *best = a.sg;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+// Launches a strip kernel with the occupancy the device allows (persistent grid).  The strip shape
+// of the level comes from the latency model (choose_strips), or from a measurement when the context
+// has autotuning on (first use of a kernel on a level size, outside stream capture) or the process
+// measured it before.
 template <class Kern, class Args>
 static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls) {
   int per_sm = 1;
-  const int rc = kernel_cfg(kern, smem, &per_sm);
+  int rc = kernel_cfg(kern, smem, &per_sm);
   if (rc) return rc;
   const long long cap = (long long)num_sms() * per_sm;
-  a.sg = choose_strips(a.g, (long long)num_sms() * 4);
-  const StripGeo& sg = a.sg;
-  const long long need = (sg.nstrips + kWarps - 1) / kWarps;
-  const int grid = (int)(need < cap ? need : cap);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!tuned_shape((const void*)kern, dev, a.g, &a.sg)) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (c->autotune && cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+      if ((rc = autotune_shape(c, kern, a, smem, cap, &a.sg))) return rc;
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      if (g_ntuned < 512)
+        g_tuned[g_ntuned++] = TunedShape{(const void*)kern, dev, a.g.nx, a.g.ny, a.g.nz, a.sg.wy, a.sg.cz};
+    } else {
+      a.sg = choose_strips(a.g, (long long)num_sms() * 4);
+    }
+  }
+  const int grid = grid_for(a.sg, cap);
   if (grid <= 0) return HPC_OK;
   if ((size_t)grid * 3 > c->partials_cap) return cuda_fail(cudaErrorInvalidValue, "partials buffer");
   timing_begin(c, cls);
@@ -422,6 +512,20 @@ static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls) {
   timing_end(c, cls);
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
+}
+
+// Shapes measured so far (for reports): up to cap entries of {nx, ny, nz, wy, cz}.
+int tuned_shapes(int* out5, int cap) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  int n = 0;
+  for (int i = 0; i < g_ntuned && n < cap; ++i, ++n) {
+    out5[5 * n + 0] = g_tuned[i].nx;
+    out5[5 * n + 1] = g_tuned[i].ny;
+    out5[5 * n + 2] = g_tuned[i].nz;
+    out5[5 * n + 3] = g_tuned[i].wy;
+    out5[5 * n + 4] = g_tuned[i].cz;
+  }
+  return n;
 }
 
 // Isotropic spacing (hx = hy = hz) selects the kernels that fold 1/h^2 into the material.

@@ -1018,6 +1018,18 @@ int hpc_sync(hpc_ctx* c) {
   return HPC_OK;
 }
 
+int hpc_set_autotune(hpc_ctx* c, int on) {
+  if (!c) return arg_fail("null context");
+  c->autotune = on != 0;
+  return HPC_OK;
+}
+
+int hpc_tuned_shapes(int* out5, int cap, int* count) {
+  if (!count || (cap > 0 && !out5)) return arg_fail("bad argument");
+  *count = tuned_shapes(out5, cap);
+  return HPC_OK;
+}
+
 int hpc_set_choice_quirk(hpc_ctx* c, int reproduce) {
   if (!c) return arg_fail("null context");
   c->choice_quirk = reproduce != 0;

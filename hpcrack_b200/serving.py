@@ -71,9 +71,14 @@ def default_footprint(w: ms.Workload) -> int:
     return Hierarchy.footprint(w.maxlevel, w.element_nb, x0=w.x_start)
 
 
-def run_request(solver, w: ms.Workload, increments: int, mech_solver: int = 0):
+def run_request(solver, w: ms.Workload, increments: int, mech_solver: int = 0, precision_mg: bool = True):
     """One fracture run on an allocated solver: material from the image, pre-crack, increments
-    (mech_solver 0: the reference's FAS cycles, 1: flexible PCG preconditioned by one V-cycle)."""
+    (mech_solver 0: the reference's FAS cycles, 1: flexible PCG preconditioned by one FP64 V-cycle,
+    2: the precision form; the flexible forms use solver.PRECISION_MG unless precision_mg is False)."""
+    from .solver import PRECISION_MG
+    mg_u = w.mg_u
+    if mech_solver != 0 and precision_mg:
+        mg_u = tuple(PRECISION_MG) + (w.mg_u[4],)
     nx, ny, nz = w.nodes
     solver.image_material(w.image, (nx, ny, nz), w.table(), w.voxel_size)
     if w.crack:
@@ -83,7 +88,7 @@ def run_request(solver, w: ms.Workload, increments: int, mech_solver: int = 0):
         solver.voigt_all_level(H_FIELD)
     outs = []
     for t in range(increments):
-        outs.append(solver.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
+        outs.append(solver.step(t, mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
                                 dU_factor=w.du_factor, mech_tol=w.mech_tol, pf_tol=w.pf_tol,
                                 mech_solver=mech_solver))
     return outs
@@ -91,13 +96,15 @@ def run_request(solver, w: ms.Workload, increments: int, mech_solver: int = 0):
 
 class SolveServer:
     def __init__(self, hbm_budget: int, slots: int, solver_factory: Callable = None,
-                 footprint: Callable = None, keep_fields: bool = False, mech_solver: int = 0):
+                 footprint: Callable = None, keep_fields: bool = False, mech_solver: int = 0,
+                 precision_mg: bool = True):
         self.budget = int(hbm_budget)
         self.slots = int(slots)
         self.factory = solver_factory or default_factory()
         self.footprint = footprint or default_footprint
         self.keep_fields = keep_fields
         self.mech_solver = int(mech_solver)
+        self.precision_mg = precision_mg
         self._cv = threading.Condition()
         self._pending: list[Request] = []
         self._closed = False
@@ -187,7 +194,7 @@ class SolveServer:
             solver = None
             try:
                 solver = self.factory(req.workload)
-                outs = run_request(solver, req.workload, req.increments, self.mech_solver)
+                outs = run_request(solver, req.workload, req.increments, self.mech_solver, self.precision_mg)
                 fields = None
                 if self.keep_fields:
                     L = req.workload.maxlevel

@@ -22,6 +22,10 @@ U, FU, RU, UOLD = 16, 17, 18, 19
 VECTOR_FIELDS = (U, FU, RU, UOLD)
 KC_MECH_PCG_FINEST, KC_PF_PCG_FINEST, KC_MECH_UPDATE_FINEST = 0, 1, 2
 MECH_FAS, MECH_FCG, MECH_MIXED = 0, 1, 2  # hpc_step_params.mech_solver
+# V-cycle (nu0, nu1, nu2, gamma) of the flexible forms' preconditioner: more post-smoothing than the
+# reference's V(4, 2) pays off once the cycle is a preconditioner (257^3 specimen, precision form:
+# V(4,2) 1.15 solves/s, V(4,4) 1.31)
+PRECISION_MG = (50, 4, 4, 1)
 
 
 def _dptr(a: np.ndarray):
@@ -120,6 +124,19 @@ class Hierarchy:
         a = np.empty(self.n(level), dtype=np.int16)
         self._c("hpc_download_choice", level, a.ctypes.data_as(C.POINTER(C.c_int16)))
         return a
+
+    def set_autotune(self, on: bool):
+        """Measure strip shapes on first use of each kernel and level size (see hpc_set_autotune)."""
+        self._c("hpc_set_autotune", int(bool(on)))
+
+    @staticmethod
+    def tuned_shapes():
+        """[(nx, ny, nz, element rows, planes)] measured so far in this process."""
+        lib = _L.load()
+        buf = (C.c_int * (5 * 512))()
+        n = C.c_int(0)
+        _L.check("hpc_tuned_shapes", lib.hpc_tuned_shapes(buf, 512, C.byref(n)))
+        return [tuple(buf[5 * i:5 * i + 5]) for i in range(n.value)]
 
     def set_choice_quirk(self, reproduce: bool):
         self._c("hpc_set_choice_quirk", int(bool(reproduce)))

@@ -114,6 +114,14 @@ const char* hpc_last_error(void);
 /* 1 (default) reproduces the reference's MP_choice loop bounds (material_selection.cpp:60-63),
  * 0 visits every element. */
 int hpc_set_choice_quirk(hpc_ctx* ctx, int reproduce);
+/* No counterpart in the reference: 1 makes this context measure the strip shape (element rows x
+ * planes per warp) of each element kernel on each level size at its first use, by timing the
+ * candidates on the live data, instead of taking the latency model's choice; measured shapes are
+ * shared by every context of the process.  Results differ from the model's shapes only in the
+ * rounding of the reductions (the grid changes); the default 0 keeps runs reproducible. */
+int hpc_set_autotune(hpc_ctx* ctx, int on);
+/* The measured shapes so far: up to cap entries {nx, ny, nz, element rows, planes}. */
+int hpc_tuned_shapes(int* out5, int cap, int* count);
 /* Kernels launched by this context since the last reset (instrumentation for benchmarks). */
 int hpc_launch_count(hpc_ctx* ctx, long long* count, int reset);
 /* The context's CUDA stream (cudaStream_t), for callers that time on it. */
