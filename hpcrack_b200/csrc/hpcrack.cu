@@ -218,6 +218,7 @@ static int pf_diags(hpc_ctx* c, int top, double lc) {
 // pcg_u (mechanical_pcg.cpp:223-330) with preMu of level l already built.  Device scalars only.
 static int pcg_u_dev(hpc_ctx* c, int l, double small_k, double Ut, int nb, int t) {
   if (nb > kMaxRelax) return arg_fail("nb_relax too large");
+  if (c->fused_coarsest && l == 0 && coarse_pcg_fits(c, l)) return launch_coarse_pcg(c, l, Ut, nb);
   LevelFields& F = c->F[l];
   int rc;
   if ((rc = launch_bc(c, l, F.u, nullptr, 0, Ut))) return rc;  // Dirichlet_BD
@@ -863,6 +864,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   c->device = device;
   c->choice_quirk = 1;
   c->use_graphs = 1;
+  c->fused_coarsest = 1;
   c->timing_class = HPC_KC_NONE;
   HostLevel lv[kMaxLevels];
   host_geometry(*geo, c->box, lv);
@@ -955,6 +957,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   shape_table(N);
   int rc = upload_shape_table(N);
   if (rc) return fail(rc);
+  if ((rc = coarse_pcg_prepare())) return fail(rc);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "create sync"));
   *out = c;
   return HPC_OK;
@@ -1015,6 +1018,12 @@ int hpc_level_dims(hpc_ctx* c, int level, int* n3, double* h3) {
 int hpc_sync(hpc_ctx* c) {
   if (!c) return arg_fail("null context");
   HPC_CUDA(cudaStreamSynchronize(c->stream));
+  return HPC_OK;
+}
+
+int hpc_set_fused_coarsest(hpc_ctx* c, int on) {
+  if (!c) return arg_fail("null context");
+  c->fused_coarsest = on != 0;
   return HPC_OK;
 }
 

@@ -106,6 +106,7 @@ struct hpc_ctx {
   } gmech, gpf, g32;  // g32: FP32 coarse part of the mixed-precision preconditioner
   int use_graphs;
   int autotune;  // measure strip shapes on first use (hpc_set_autotune)
+  int fused_coarsest;  // coarse-level pcg_u in one block when the level fits (hpc_set_fused_coarsest)
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
@@ -278,6 +279,10 @@ int launch_choice_level(hpc_ctx* c, int level, double small_k, bool do_choice, b
 int launch_crack(hpc_ctx* c, int level, const uint8_t* fx, const uint8_t* fy, const uint8_t* fz, double Hc);
 int launch_zero_count(hpc_ctx* c, int level, int ncomp, const double* v, int slot);
 int upload_shape_table(const double* N64);
+// Whole coarse-level pcg_u in one thread block (coarse_kernels.cu), for levels small enough
+bool coarse_pcg_fits(hpc_ctx* c, int level);
+int coarse_pcg_prepare();
+int launch_coarse_pcg(hpc_ctx* c, int level, double Ut, int nb);
 int tuned_shapes(int* out5, int cap);  // measured strip shapes: {nx, ny, nz, wy, cz} per entry
 
 }  // namespace hpc

@@ -125,6 +125,10 @@ class Hierarchy:
         self._c("hpc_download_choice", level, a.ctypes.data_as(C.POINTER(C.c_int16)))
         return a
 
+    def set_fused_coarsest(self, on: bool):
+        """Coarsest-level pcg_u in one thread block (default) or as per-iteration kernels."""
+        self._c("hpc_set_fused_coarsest", int(bool(on)))
+
     def set_autotune(self, on: bool):
         """Measure strip shapes on first use of each kernel and level size (see hpc_set_autotune)."""
         self._c("hpc_set_autotune", int(bool(on)))

@@ -122,6 +122,11 @@ int hpc_set_choice_quirk(hpc_ctx* ctx, int reproduce);
 int hpc_set_autotune(hpc_ctx* ctx, int on);
 /* The measured shapes so far: up to cap entries {nx, ny, nz, element rows, planes}. */
 int hpc_tuned_shapes(int* out5, int cap, int* count);
+/* No counterpart in the reference: 1 (default) runs pcg_u on the coarsest level (mechanical_pcg.cpp:
+ * 223-330 as called by mechanical_multigrid.cpp:29-32) in one thread block when the level fits in
+ * shared memory (up to about 10^3 nodes); 0 uses the per-iteration kernels.  The two differ only in
+ * the order of the same sums. */
+int hpc_set_fused_coarsest(hpc_ctx* ctx, int on);
 /* Kernels launched by this context since the last reset (instrumentation for benchmarks). */
 int hpc_launch_count(hpc_ctx* ctx, long long* count, int reset);
 /* The context's CUDA stream (cudaStream_t), for callers that time on it. */

@@ -37,6 +37,18 @@ def test_pcg_u_single(level, t):
         assert abs(fn_g - fn_o) <= 1e-12 * max(abs(fn_o), 1.0)
 
 
+@pytest.mark.parametrize("fused", [True, False])
+def test_coarsest_pcg_u_fused_and_per_iteration(fused):
+    """The coarsest-level smoother as one thread block (default) and as per-iteration kernels both
+    match the oracle; 50 iterations as the V-cycle runs them."""
+    gpu, orc = _pair(1, (8, 8, 8))
+    gpu.set_fused_coarsest(fused)
+    _, fn_g = gpu.pcg_u(0, 1e-5, 1.0, 50, 1, 0.0)
+    _, fn_o = orc.pcg_u(0, 1e-5, 1.0, 50, 1, 0.0)
+    # after 50 iterations the residual is at rounding level, so only u is compared
+    assert rel(gpu.get(U, 0), orc.get(U, 0)) < 1e-10
+
+
 def test_pcg_d_single():
     gpu, orc = _pair(1, (8, 8, 8))
     for impl in (gpu, orc):
