@@ -33,7 +33,10 @@ if ROOT not in sys.path:
 METRIC = "MDoF-iter/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
-PCG_APPLY_BYTES_PER_NODE = 73
+# Algorithmic bytes per finest node of the PCG apply during a mechanical solve: p and w (24 B each)
+# and the precomputed Gauss-point moduli K_g, G_g (16 doubles per element = 128 B).  (The nodal
+# form that interpolates K, G, d and the regime in the apply itself reads 73 B/node.)
+PCG_APPLY_BYTES_PER_NODE = 176
 MECH_SOLVERS = {"fas": 0, "fcg": 1, "mixed": 2}
 
 # DRAM bytes (read + write) per launch of the finest PCG apply: the ncu capture of
@@ -111,10 +114,11 @@ def run_serving(args, local):
             q.workload.mg_u = v + (q.workload.mg_u[4],)
     srv = sv.SolveServer(budget, args.slots, solver_factory=sv.default_factory(local),
                          mech_solver=MECH_SOLVERS[args.mech_solver], precision_mg=not args.mg_u)
-    from hpcrack_b200.solver import PRECISION_MG
+    from hpcrack_b200.solver import precision_mg
     mg_used = reqs[0].workload.mg_u
     if args.mech_solver != "fas" and not args.mg_u:
-        mg_used = tuple(PRECISION_MG) + (mg_used[4],)
+        mg_used = "per request: " + ", ".join(sorted({str(precision_mg(q.workload.maxlevel, q.workload.element_nb,
+                                                                        q.workload.mg_u[4])) for q in reqs}))
     t0 = time.perf_counter()
     res = srv.replay(reqs)
     wall = time.perf_counter() - t0
@@ -127,7 +131,8 @@ def run_serving(args, local):
             "dtype": "f64", "data": "synthetic", "config": {"workload": form, "slots": args.slots,
                                                             "hbm_budget_gb": args.hbm_budget_gb,
                                                             "mech_solver": args.mech_solver,
-                                                            "mg_u": list(mg_used)},
+                                                            "mg_u": mg_used if isinstance(mg_used, str)
+                                                            else list(mg_used)},
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "wall_s": wall,
             "mdof_iter_per_s": dof_iters / wall / 1e6, "peak_active": srv.peak_active,
             "peak_hbm_gb": srv.peak_used / (1 << 30)}
@@ -414,15 +419,14 @@ def run_b200(args, rank, world, local):
     max_ms, tot_dof_iters = replicas.aggregate(ms_total, dof_iters, world)
     value = tot_dof_iters / (max_ms / 1e3) / 1e6
 
-    # roofline of the dominant kernel: the finest-level PCG apply w = K(d) p with the (p, w) reduction.
-    # Algorithmic bytes per finest node: p read and w written (3 x 8 B each), bulK, G, d read (8 B each),
-    # regime byte read = 73 B.
+    # roofline of the dominant kernel: the finest-level PCG apply w = K(d) p with the (p, w) reduction
+    # (PCG_APPLY_BYTES_PER_NODE algorithmic bytes per finest node).
     roofline = None
     if kn > 0:
         bytes_total = N * PCG_APPLY_BYTES_PER_NODE * kn
         achieved = bytes_total / (kms / 1e3) / 1e9
         peak, src = peaks()
-        roofline = {"bound": "hbm", "kernel": "mech_kernel<finest, PCG> (w = K(d) p, (p, w))",
+        roofline = {"bound": "hbm", "kernel": "mech_kernel<finest, PCG, Gauss-point moduli> (w = K(d) p, (p, w))",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "peak_source": src, "traffic": PCG_APPLY_TRAFFIC_PER_NODE * N,
                     "traffic_note": "bytes per launch: ncu dram bytes per node of the 193^3 capture x nodes",
@@ -483,8 +487,8 @@ def run_b200(args, rank, world, local):
     forms = None
     if not args.no_forms and args.mech_solver == "fas":
         wp = workload(args)
-        from hpcrack_b200.solver import PRECISION_MG
-        wp.mg_u = tuple(PRECISION_MG) + (wp.mg_u[4],)
+        from hpcrack_b200.solver import precision_mg
+        wp.mg_u = precision_mg(wp.maxlevel, wp.element_nb, wp.mg_u[4])
         hp = load_specimen(wp, local)
         sp = torch.cuda.ExternalStream(hp.stream())
 

@@ -16,6 +16,7 @@
 // list (persistent grid).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "device_common.cuh"
@@ -137,6 +138,7 @@ struct MechKT {
   int set_fnorm;
   const T* invM;
   const T* rf;
+  const T* gpm;  // finest level, precomputed Gauss-point moduli: K at [g * n + e], G at [(8 + g) * n + e]
   RedTarget red;
 };
 using MechK = MechKT<double>;
@@ -181,10 +183,12 @@ __device__ __forceinline__ void mech_moduli_finest(const T (&Kn)[8], const T (&G
 }
 
 // T = double: the plain form; T = float: the precision form's V-cycle (reductions stay FP64).
-template <typename T, bool FINEST, int EPI, bool DIAG, bool ISO>
+// GPM: the finest level's Gauss-point moduli come precomputed (gp_material_kernel) instead of being
+// interpolated from the staged nodal K, G, d in every apply.
+template <typename T, bool FINEST, int EPI, bool DIAG, bool ISO, bool GPM = false>
 __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
   constexpr int NU = DIAG ? 0 : 3;
-  constexpr int NF = NU + (FINEST ? 3 : 2);
+  constexpr int NF = NU + (FINEST ? (GPM ? 0 : 3) : 2);
   extern __shared__ __align__(16) unsigned char mech_smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   T* ring = reinterpret_cast<T*>(mech_smem) + (size_t)wib * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32);
@@ -243,7 +247,14 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
         T Kw[8], Gw[8];
         // ISO: the 1/h^2 of the two gradients goes into the Gauss weight (see sf_forward)
         const T wg = ISO ? T(k.g.wg) * (s.ih[0] * s.ih[0]) : T(k.g.wg);
-        if (FINEST) {
+        if (FINEST && GPM) {
+          const long long e = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
+#pragma unroll
+          for (int g = 0; g < 8; ++g) {
+            Kw[g] = k.gpm[(long long)g * k.g.n + e];
+            Gw[g] = k.gpm[(long long)(8 + g) * k.g.n + e];
+          }
+        } else if (FINEST) {
           T Kn[8], Gn[8], dn[8];
 #pragma unroll
           for (int n = 0; n < 8; ++n) {
@@ -533,9 +544,17 @@ inline bool iso(const LevelGeo& g) { return g.hx == g.hy && g.hy == g.hz; }
 
 template <bool F, int E, bool D, typename T = double>
 static int run_mech(hpc_ctx* c, const MechKT<T>& k) {
+  const int cls = (F && E == EPI_PCG && !D && sizeof(T) == 8) ? HPC_KC_MECH_PCG_FINEST : HPC_KC_NONE;
+  if constexpr (F && !D) {
+    if (k.gpm) {  // precomputed Gauss-point moduli: only u is staged
+      constexpr int NF = 3;
+      const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
+      if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true, true>, k, smem, cls);
+      return launch_strips(c, mech_kernel<T, F, E, D, false, true>, k, smem, cls);
+    }
+  }
   constexpr int NF = (D ? 0 : 3) + (F ? 3 : 2);
   const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
-  const int cls = (F && E == EPI_PCG && !D && sizeof(T) == 8) ? HPC_KC_MECH_PCG_FINEST : HPC_KC_NONE;
   if constexpr (!D) {
     if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true>, k, smem, cls);
   }
@@ -571,6 +590,7 @@ int launch_mech(hpc_ctx* c, const MechCall& m) {
   k.set_fnorm = m.set_fnorm;
   k.invM = m.invM;
   k.rf = m.rf;
+  k.gpm = (m.finest && c->gpm_active) ? c->F[m.level].gpm : nullptr;
   k.red = make_red(c, m.s_out0, m.s_out1, m.s_out2);
   const bool f = m.finest;
   switch (m.epi) {
@@ -622,6 +642,7 @@ int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
   k.set_fnorm = 0;
   k.invM = m.invM;
   k.rf = m.rf;
+  k.gpm = (m.finest && c->gpm_active) ? F.gpm : nullptr;
   k.red = make_red(c, m.s_out0, m.s_out1, m.s_out2);
   const bool fin = m.finest;
   switch (m.epi) {
@@ -633,6 +654,48 @@ int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
     case EPI_FAS: return run_mech<false, EPI_FAS, false>(c, k);
   }
   return HPC_ERR_ARG;
+}
+
+// Gauss-point moduli of the finest level, computed once per mechanical solve (the material is
+// fixed while the solve runs): the same mech_moduli_finest as the strip kernels, so the applies that
+// read them produce the same bits as the applies that interpolate the nodal fields themselves.
+template <typename T>
+__global__ void gp_material_kernel(LevelGeo g, const T* K, const T* G, const T* d, const int8_t* choice,
+                                   double small_k, T* gpm) {
+  const SFt<T> s = make_sf<T>(g);
+  const bool isotropic = g.hx == g.hy && g.hy == g.hz;
+  const T wg = isotropic ? T(g.wg) * (s.ih[0] * s.ih[0]) : T(g.wg);
+  const long long ne = (long long)(g.nx - 1) * (g.ny - 1) * (g.nz - 1);
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < ne; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % (g.nx - 1)), j = (int)((q / (g.nx - 1)) % (g.ny - 1)), kz = (int)(q / ((long long)(g.nx - 1) * (g.ny - 1)));
+    T Kn[8], Gn[8], dn[8], Kw[8], Gw[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const long long o = nidx(g, i + (n & 1), j + ((n >> 1) & 1), kz + (n >> 2));
+      Kn[n] = K[o];
+      Gn[n] = G[o];
+      dn[n] = d[o];
+    }
+    const long long e = nidx(g, i, j, kz);
+    mech_moduli_finest(Kn, Gn, dn, choice[e], T(small_k), wg, s, Kw, Gw);
+#pragma unroll
+    for (int q8 = 0; q8 < 8; ++q8) {
+      gpm[(long long)q8 * g.n + e] = Kw[q8];
+      gpm[(long long)(8 + q8) * g.n + e] = Gw[q8];
+    }
+  }
+}
+
+int launch_gp_material(hpc_ctx* c, double small_k) {
+  const int L = c->maxlevel;
+  const LevelGeo& g = c->L[L];
+  const LevelFields& F = c->F[L];
+  const long long ne = (long long)(g.nx - 1) * (g.ny - 1) * (g.nz - 1);
+  const int grid = (int)std::min<long long>((ne + 255) / 256, (long long)num_sms() * 8);
+  if (grid <= 0) return HPC_OK;
+  gp_material_kernel<double><<<grid, 256, 0, c->stream>>>(g, F.bulK, F.G, F.d, F.choice, small_k, F.gpm);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
 }
 
 // ------------------------------------------------------------------------------------------

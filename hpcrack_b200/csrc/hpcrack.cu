@@ -443,6 +443,22 @@ static int mech_material(hpc_ctx* c, double small_k) {
   return HPC_OK;
 }
 
+// Gauss-point moduli of the finest level for the solve about to run; while the returned scope lives,
+// the finest applies read them (the material does not change during a mechanical solve).
+struct GpmScope {
+  hpc_ctx* c;
+  explicit GpmScope(hpc_ctx* ctx) : c(ctx) {}
+  ~GpmScope() { c->gpm_active = 0; }
+};
+static int gp_material(hpc_ctx* c, double small_k) {
+  LevelFields& F = c->F[c->maxlevel];
+  if (!F.gpm) HPC_CUDA(cudaMalloc((void**)&F.gpm, sizeof(double) * 16 * (size_t)c->L[c->maxlevel].n));
+  int rc = launch_gp_material(c, small_k);
+  if (rc) return rc;
+  c->gpm_active = 1;
+  return HPC_OK;
+}
+
 // u_entire (mechanical_displacement.cpp:25-115).
 static int u_entire_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, double mech_tol, int* cycles,
                         long long* fin_iters) {
@@ -451,6 +467,8 @@ static int u_entire_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut,
   if ((rc = write_scalar(c, S_FNORM, c->f_norm))) return rc;
   if ((rc = mech_material(c, small_k))) return rc;
   if ((rc = mech_diags(c, L, small_k))) return rc;
+  GpmScope gpm_scope(c);
+  if (L > 0 && (rc = gp_material(c, small_k))) return rc;
   // Initial_residual_u (mechanical_pcg.cpp:193-220): no Dirichlet_BD on u, no reaction copy
   MechCall m{};
   m.level = L;
@@ -517,6 +535,10 @@ static int ensure_f32(hpc_ctx* c) {
     float** mat_f[] = {&F.K, &F.G, &F.d};
     float** mat_c[] = {&F.Ke, &F.Ge};
     const bool fin = (l == c->maxlevel);
+    if (fin && l > 0) {
+      HPC_CUDA(cudaMalloc((void**)&F.gpm, 16 * n * sizeof(float)));
+      HPC_CUDA(cudaMemsetAsync(F.gpm, 0, 16 * n * sizeof(float), c->stream));
+    }
     for (int q = 0; q < (fin ? 3 : 2); ++q) {
       float** p = fin ? mat_f[q] : mat_c[q];
       HPC_CUDA(cudaMalloc((void**)p, n * sizeof(float)));
@@ -538,6 +560,7 @@ static int f32_material(hpc_ctx* c) {
       if ((rc = launch_to_f32(c, F.bulK, G.K, n))) return rc;
       if ((rc = launch_to_f32(c, F.G, G.G, n))) return rc;
       if ((rc = launch_to_f32(c, F.d, G.d, n))) return rc;
+      if (c->gpm_active && G.gpm && (rc = launch_to_f32(c, F.gpm, G.gpm, 16 * n))) return rc;
     } else {
       if ((rc = launch_to_f32(c, F.Ke, G.Ke, n))) return rc;
       if ((rc = launch_to_f32(c, F.Ge, G.Ge, n))) return rc;
@@ -671,6 +694,8 @@ static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double
   if ((rc = write_scalar(c, S_FNORM, c->f_norm))) return rc;
   if ((rc = mech_material(c, small_k))) return rc;
   if ((rc = mech_diags(c, L, small_k))) return rc;
+  GpmScope gpm_scope(c);
+  if (L > 0 && (rc = gp_material(c, small_k))) return rc;
   if (mixed) {
     if ((rc = ensure_f32(c))) return rc;
     if ((rc = f32_material(c))) return rc;
@@ -839,8 +864,17 @@ int hpc_footprint(const hpc_geometry* geo, size_t* bytes) {
     total += level_bytes(n) + (size_t)(lv[l].nx + lv[l].ny + lv[l].nz);
   }
   const HostLevel& f = lv[geo->maxlevel];
-  total += (size_t)f.px * f.ny * f.nz * sizeof(double);  // d_old
+  const size_t nf = (size_t)f.px * f.ny * f.nz;
+  total += nf * sizeof(double);  // d_old
   total += sizeof(double) * (kScalarPool + 3 * 8192) + 64;
+  // allocated on first use: Gauss-point moduli (16 n), flexible-PCG vectors (5 x 3n), the FP32
+  // mirror of every level (7 x 3n + material) with its Gauss-point moduli, the checkpoint (6 dense)
+  total += nf * sizeof(double) * (16 + 15);
+  for (int l = 0; l <= geo->maxlevel; ++l) {
+    const size_t n = (size_t)lv[l].px * lv[l].ny * lv[l].nz;
+    total += n * sizeof(float) * (21 + (l == geo->maxlevel ? 3 + 16 : 2));
+  }
+  total += 6 * (size_t)f.nx * f.ny * f.nz * sizeof(double);
   *bytes = total;
   return HPC_OK;
 }
@@ -970,7 +1004,7 @@ int hpc_destroy(hpc_ctx* c) {
   for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
     LevelFields& F = c->F[l];
     void* ptrs[] = {F.bulK, F.G, F.gc, F.d, F.H, F.fd, F.Ke, F.Ge, F.R, F.dold, F.preMd, F.pd, F.wd, F.tmp1,
-                    F.u, F.fu, F.ru, F.uold, F.preMu, F.p, F.w, F.tmp3, F.choice};
+                    F.u, F.fu, F.ru, F.uold, F.preMu, F.p, F.w, F.tmp3, F.choice, F.gpm};
     for (void* p : ptrs)
       if (p) cudaFree(p);
   }
@@ -991,7 +1025,7 @@ int hpc_destroy(hpc_ctx* c) {
   }
   for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
     LevelF32& G = c->F32[l];
-    float* fa[] = {G.u, G.fu, G.ru, G.uold, G.p, G.w, G.invM, G.K, G.G, G.d, G.Ke, G.Ge};
+    float* fa[] = {G.u, G.fu, G.ru, G.uold, G.p, G.w, G.invM, G.K, G.G, G.d, G.Ke, G.Ge, G.gpm};
     for (float* p : fa)
       if (p) cudaFree(p);
   }

@@ -40,6 +40,7 @@ struct LevelFields {
   double *preMu, *p, *w, *tmp3;  // 3n; preMu holds the inverse diagonal while a solve runs
   double *preMd, *pd, *wd, *tmp1;  // n;  preMd likewise
   uint8_t* bc_host_copy;           // host copies of the axis flags (nx+ny+nz bytes)
+  double* gpm;  // finest level: Gauss-point moduli of the running mechanical solve, 16n (first use)
 };
 
 // Single-precision mirror of one level for the V-cycle of the precision form (hpc_step with
@@ -48,6 +49,7 @@ struct LevelF32 {
   float *u, *fu, *ru, *uold, *p, *w, *invM;  // 3n each; invM: inverse diagonal of K
   float *K, *G, *d;                           // finest level: nodal moduli and phase field
   float *Ke, *Ge;                             // coarse levels: element moduli
+  float* gpm;                                 // finest level: Gauss-point moduli, 16n
 };
 
 // Device scalar pool layout (doubles).
@@ -107,6 +109,7 @@ struct hpc_ctx {
   int use_graphs;
   int autotune;  // measure strip shapes on first use (hpc_set_autotune)
   int fused_coarsest;  // coarse-level pcg_u in one block when the level fits (hpc_set_fused_coarsest)
+  int gpm_active;      // finest applies read F[maxlevel].gpm (set while a mechanical solve runs)
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
@@ -183,6 +186,8 @@ struct MechCall {
 };
 int launch_mech(hpc_ctx* c, const MechCall& m);
 int launch_mech_diag(hpc_ctx* c, int level, bool finest, double small_k, double* out);
+// Gauss-point moduli of the finest level into F[maxlevel].gpm (from bulK, G, d and the regimes)
+int launch_gp_material(hpc_ctx* c, double small_k);
 
 // Single-precision operator on the FP32 mirror of a level (EPI_PLAIN, EPI_RESIDUAL, EPI_PCG, EPI_FAS);
 // the residual zeroes Dirichlet rows and sums (r, M^-1 r) into s_out1 and |r|^2 into s_out2 in FP64.

@@ -74,11 +74,12 @@ def default_footprint(w: ms.Workload) -> int:
 def run_request(solver, w: ms.Workload, increments: int, mech_solver: int = 0, precision_mg: bool = True):
     """One fracture run on an allocated solver: material from the image, pre-crack, increments
     (mech_solver 0: the reference's FAS cycles, 1: flexible PCG preconditioned by one FP64 V-cycle,
-    2: the precision form; the flexible forms use solver.PRECISION_MG unless precision_mg is False)."""
-    from .solver import PRECISION_MG
+    2: the precision form; the flexible forms use solver.precision_mg's cycle unless precision_mg is
+    False)."""
+    from .solver import precision_mg as _precision_mg
     mg_u = w.mg_u
     if mech_solver != 0 and precision_mg:
-        mg_u = tuple(PRECISION_MG) + (w.mg_u[4],)
+        mg_u = _precision_mg(w.maxlevel, w.element_nb, w.mg_u[4])
     nx, ny, nz = w.nodes
     solver.image_material(w.image, (nx, ny, nz), w.table(), w.voxel_size)
     if w.crack:

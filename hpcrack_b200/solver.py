@@ -26,6 +26,28 @@ MECH_FAS, MECH_FCG, MECH_MIXED = 0, 1, 2  # hpc_step_params.mech_solver
 # reference's V(4, 2) pays off once the cycle is a preconditioner (257^3 specimen, precision form:
 # V(4,2) 1.15 solves/s, V(4,4) 1.31)
 PRECISION_MG = (50, 4, 4, 1)
+# Coarsest iterations when the coarsest level is too large for the one-block solver: there each
+# iteration costs three launches, and a 20-iteration coarse solve is the better preconditioner per
+# unit time (64-specimen mix: 50 iterations 4.2-4.8 solves/s, 20 iterations 5.9; 10 iterations 2.3).
+# With a one-block coarsest solve (e.g. 9^3 under a 257^3 specimen) 50 stays best (1.35 vs 0.84).
+PRECISION_NU0_LARGE_COARSEST = 20
+
+
+def coarsest_in_one_block(maxlevel: int, element_nb) -> bool:
+    """Whether the library solves the coarsest level in one thread block (the rule of
+    coarse_pcg_fits in coarse_kernels.cu: 15 N + 26 E + 33 doubles of shared memory, at most 220 KiB,
+    and a coarsest level below the finest)."""
+    e = [int(v) for v in element_nb]
+    n_nodes = (e[0] + 1) * (e[1] + 1) * (e[2] + 1)
+    n_elem = e[0] * e[1] * e[2]
+    return maxlevel >= 1 and 8 * (15 * n_nodes + 26 * n_elem + 33) <= 220 * 1024
+
+
+def precision_mg(maxlevel: int, element_nb, ncy: int) -> tuple:
+    """The flexible forms' preconditioner cycle for a hierarchy (PRECISION_MG, with fewer coarsest
+    iterations when the coarsest level does not fit one thread block)."""
+    nu0 = PRECISION_MG[0] if coarsest_in_one_block(maxlevel, element_nb) else PRECISION_NU0_LARGE_COARSEST
+    return (nu0,) + tuple(PRECISION_MG[1:]) + (int(ncy),)
 
 
 def _dptr(a: np.ndarray):

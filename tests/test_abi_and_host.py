@@ -53,7 +53,9 @@ def test_footprint_and_bad_geometry():
     b = C.c_size_t(0)
     assert lib.hpc_footprint(C.byref(g), C.byref(b)) == 0
     n = 260 * 257 * 257  # padded finest slots of 257^3
-    assert 38 * 8 * n < b.value < 60 * 8 * n
+    # ~38 doubles per finest node allocated at creation (+1/7 for the coarse levels), plus what the
+    # flexible forms, the Gauss-point moduli and a checkpoint allocate on first use (~55 more)
+    assert 80 * 8 * n < b.value < 120 * 8 * n
     bad = L.hpc_geometry(-1, (C.c_int * 3)(8, 8, 8), (C.c_double * 3)(0, 0, 0), (C.c_int * 3)(0, 0, 0))
     assert lib.hpc_footprint(C.byref(bad), C.byref(b)) == 1
 
