@@ -40,10 +40,10 @@ PCG_APPLY_BYTES_PER_NODE = 176
 MECH_SOLVERS = {"fas": 0, "fcg": 1, "mixed": 2}
 
 # DRAM bytes (read + write) per launch of the finest PCG apply: the ncu capture of
-# profiles/mech_pcg_apply_mid193.md measured 440.5 MB + 153.1 MB on the 193^3 level (7,189,057 nodes,
-# 82.6 B/node); other sizes scale that per-node figure by their node count (traffic grows with the
-# nodes, the strip-edge re-reads included).
-PCG_APPLY_TRAFFIC_PER_NODE = (440.516864e6 + 153.093120e6) / 193 ** 3
+# profiles/mech_pcg_apply_mid193.md measured 1339.8 MB + 165.9 MB on the 193^3 level (7,189,057
+# nodes, 209.4 B/node: the Gauss-point moduli of strip-edge elements are read twice); other sizes
+# scale that per-node figure by their node count.
+PCG_APPLY_TRAFFIC_PER_NODE = (1339.779e6 + 165.902848e6) / 193 ** 3
 
 
 def parse_args():
