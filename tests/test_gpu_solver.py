@@ -80,7 +80,7 @@ def test_cycles():
     assert rel(gpu.get(D, 2), orc.get(D, 2)) < 1e-10
 
 
-@pytest.mark.parametrize("name,steps", [("small17", 4), ("small33", 3)])
+@pytest.mark.parametrize("name,steps", [("small17", 4), ("small33", 3), ("parity65", 3)])
 def test_staggered_steps(name, steps):
     w = ms.make_workload(name)
     gpu = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start)
@@ -101,6 +101,25 @@ def test_staggered_steps(name, steps):
         assert rel(gpu.get(H, L), orc.get(H, L)) < 1e-10, t
         assert abs(og[1] - oo[1]) <= 1e-10 * max(abs(oo[1]), 1e-300), t
         assert abs(og[3] - oo[3]) <= 1e-10 * max(abs(oo[3]), 1e-300), t
+
+
+def test_parity65_at_its_tolerance():
+    """The 65^3 configuration as specified: three increments of 1e-4*Nz solved to |r|/|f| <= 1e-8
+    (squared 1e-16); V-cycle counts equal and u, d, H within 1e-10 of the oracle."""
+    w = ms.make_workload("parity65")
+    gpu = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start)
+    orc = COracle(w.maxlevel, w.element_nb, x0=w.x_start)
+    load_workload([gpu, orc], w)
+    L = w.maxlevel
+    for t in range(w.increments):
+        og = gpu.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
+                      mech_tol=w.mech_tol, pf_tol=w.pf_tol)
+        oo = orc.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
+                      mech_tol=w.mech_tol, pf_tol=w.pf_tol)
+        assert og[4] == oo[4] and og[5] == oo[5], (t, og, oo)
+        assert og[6] == oo[6] and og[7] == oo[7], (t, og, oo)  # finest smoother iterations
+        for f in (U, D, H):
+            assert rel(gpu.get(f, L), orc.get(f, L)) < 1e-10, (t, f)
 
 
 def test_reference_schedule_Ue():
