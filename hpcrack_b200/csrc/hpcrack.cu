@@ -452,7 +452,11 @@ struct GpmScope {
 };
 static int gp_material(hpc_ctx* c, double small_k) {
   LevelFields& F = c->F[c->maxlevel];
-  if (!F.gpm) HPC_CUDA(cudaMalloc((void**)&F.gpm, sizeof(double) * 16 * (size_t)c->L[c->maxlevel].n));
+  if (!F.gpm) {
+    const size_t bytes = sizeof(double) * 16 * (size_t)c->L[c->maxlevel].n;
+    HPC_CUDA(cudaMalloc((void**)&F.gpm, bytes));
+    HPC_CUDA(cudaMemsetAsync(F.gpm, 0, bytes, c->stream));  // non-element slots stay zero
+  }
   int rc = launch_gp_material(c, small_k);
   if (rc) return rc;
   c->gpm_active = 1;
@@ -899,6 +903,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   c->choice_quirk = 1;
   c->use_graphs = 1;
   c->fused_coarsest = 1;
+  c->f32_pairs = 1;
   c->timing_class = HPC_KC_NONE;
   HostLevel lv[kMaxLevels];
   host_geometry(*geo, c->box, lv);
@@ -1052,6 +1057,12 @@ int hpc_level_dims(hpc_ctx* c, int level, int* n3, double* h3) {
 int hpc_sync(hpc_ctx* c) {
   if (!c) return arg_fail("null context");
   HPC_CUDA(cudaStreamSynchronize(c->stream));
+  return HPC_OK;
+}
+
+int hpc_set_f32_pairs(hpc_ctx* c, int on) {
+  if (!c) return arg_fail("null context");
+  c->f32_pairs = on != 0;
   return HPC_OK;
 }
 

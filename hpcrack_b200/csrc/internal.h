@@ -110,6 +110,7 @@ struct hpc_ctx {
   int autotune;  // measure strip shapes on first use (hpc_set_autotune)
   int fused_coarsest;  // coarse-level pcg_u in one block when the level fits (hpc_set_fused_coarsest)
   int gpm_active;      // finest applies read F[maxlevel].gpm (set while a mechanical solve runs)
+  int f32_pairs;       // FP32 operator with two elements per lane (hpc_set_f32_pairs)
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
