@@ -59,8 +59,6 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-timing", action="store_true")
-    ap.add_argument("--f32-single", action="store_true",
-                    help="precision form with the one-element FP32 operator instead of the paired FP32x2 one")
     ap.add_argument("--autotune", action="store_true",
                     help="measure the element kernels' strip shapes on first use (hpc_set_autotune) instead of "
                          "the latency model's choice")
@@ -168,8 +166,6 @@ def run_profile_cycles(args, local):
     from hpcrack_b200 import microstructure as ms
     w = workload(args)
     hier = load_specimen(w, local)
-    if args.f32_single:
-        hier.set_f32_pairs(False)
     K = args.profile_cycles
     mg_u = tuple(w.mg_u[:4]) + (K,)
     mg_d = tuple(w.mg_d[:4]) + (K,)
@@ -379,8 +375,6 @@ def run_b200(args, rank, world, local):
     hier = load_specimen(w, local)
     if args.autotune:
         hier.set_autotune(True)
-    if args.f32_single:
-        hier.set_f32_pairs(False)
     stream = torch.cuda.ExternalStream(hier.stream())
 
     solver = MECH_SOLVERS[args.mech_solver]
@@ -496,8 +490,6 @@ def run_b200(args, rank, world, local):
         from hpcrack_b200.solver import precision_mg
         wp.mg_u = precision_mg(wp.maxlevel, wp.element_nb, wp.mg_u[4])
         hp = load_specimen(wp, local)
-        if args.f32_single:
-            hp.set_f32_pairs(False)
         sp = torch.cuda.ExternalStream(hp.stream())
 
         def pstep(tt):
@@ -538,6 +530,7 @@ def run_b200(args, rank, world, local):
                 "strip_shapes": ({"autotuned": [list(x) for x in Hierarchy.tuned_shapes()]} if args.autotune
                                  else "latency model (choose_strips)"),
                 "solves_per_s": world * args.steps / (max_ms / 1e3),
+                "v_cycles_per_s": world * sum(o[4] + o[5] for o in outs) / (max_ms / 1e3),
                 "steps_detail": [{"t": t_first + i, "mech_cycles": int(o[4]), "pf_cycles": int(o[5]),
                                   "mech_iters": int(o[6]), "pf_iters": int(o[7]), "F": o[1], "dmax": o[3]}
                                  for i, o in enumerate(outs)]}

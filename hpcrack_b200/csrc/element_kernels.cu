@@ -616,9 +616,6 @@ int launch_mech_diag(hpc_ctx* c, int level, bool finest, double small_k, double*
   return finest ? run_mech<true, EPI_PLAIN, true>(c, k) : run_mech<false, EPI_PLAIN, true>(c, k);
 }
 
-template <bool F, int E>
-static int run_x2(hpc_ctx* c, const MechKT<float>& k);
-
 // Single-precision element operator of the precision form's V-cycle: the same kernels on the FP32
 // mirror of a level (LevelF32); residual, PCG apply and FAS right-hand side epilogues.
 int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
@@ -648,15 +645,6 @@ int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
   k.gpm = (m.finest && c->gpm_active) ? F.gpm : nullptr;
   k.red = make_red(c, m.s_out0, m.s_out1, m.s_out2);
   const bool fin = m.finest;
-  if (c->f32_pairs && (!fin || k.gpm)) {  // paired-element kernel: coarse levels, finest with moduli
-    switch (m.epi) {
-      case EPI_PLAIN: return fin ? run_x2<true, EPI_PLAIN>(c, k) : run_x2<false, EPI_PLAIN>(c, k);
-      case EPI_RESIDUAL: return fin ? run_x2<true, EPI_RESIDUAL>(c, k) : run_x2<false, EPI_RESIDUAL>(c, k);
-      case EPI_PCG: return fin ? run_x2<true, EPI_PCG>(c, k) : run_x2<false, EPI_PCG>(c, k);
-      case EPI_FAS: return run_x2<false, EPI_FAS>(c, k);
-    }
-    return HPC_ERR_ARG;
-  }
   switch (m.epi) {
     case EPI_PLAIN:
       return fin ? run_mech<true, EPI_PLAIN, false>(c, k) : run_mech<false, EPI_PLAIN, false>(c, k);
@@ -708,288 +696,6 @@ int launch_gp_material(hpc_ctx* c, double small_k) {
   gp_material_kernel<double><<<grid, 256, 0, c->stream>>>(g, F.bulK, F.G, F.d, F.choice, small_k, F.gpm);
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
-}
-
-// ------------------------------------------------------------------------------------------
-// Precision form: the single-precision operator with two x-adjacent elements per lane, computed
-// together with the packed FP32x2 instructions of sm_100 (one instruction, two elements).  A warp
-// covers 64 node columns (x0-2 .. x0+61, plus x0+62 staged by lane 31) and outputs 62: lane l holds
-// columns c0 = x0-2+2l and c1 = c0+1 and computes elements E0 = [c0, c1] (in .x) and E1 = [c1, c1+1]
-// (in .y); node c1 = E0 corner a=1 + E1 corner a=0 inside the lane, node c0 = E0 corner a=0 + the
-// left lane's E1 corner a=1 through one shuffle.  Staging, index work and shuffles - which bound
-// the one-element FP32 kernel by instruction issue - are shared by the two elements.
-// ------------------------------------------------------------------------------------------
-// In its own namespace so that fma(double, ...) elsewhere in hpc still finds the standard overloads;
-// the sum-factorised templates reach these operators by argument-dependent lookup.
-namespace packed {
-struct F2 {
-  float2 v;
-  __device__ __forceinline__ F2() {}
-  __device__ __forceinline__ explicit F2(double a) : v(make_float2((float)a, (float)a)) {}
-  __device__ __forceinline__ explicit F2(float a) : v(make_float2(a, a)) {}
-  __device__ __forceinline__ explicit F2(int a) : v(make_float2((float)a, (float)a)) {}
-  __device__ __forceinline__ F2(float a, float b) : v(make_float2(a, b)) {}
-  __device__ __forceinline__ F2& operator+=(F2 o) {
-    v = __fadd2_rn(v, o.v);
-    return *this;
-  }
-};
-__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
-  F2 r;
-  r.v = __fadd2_rn(a.v, b.v);
-  return r;
-}
-__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
-  F2 r;
-  r.v = __ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v);
-  return r;
-}
-__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
-  F2 r;
-  r.v = __fmul2_rn(a.v, b.v);
-  return r;
-}
-__device__ __forceinline__ F2 fma(F2 a, F2 b, F2 c) {
-  F2 r;
-  r.v = __ffma2_rn(a.v, b.v, c.v);
-  return r;
-}
-}  // namespace packed
-using packed::F2;
-
-constexpr int kOX2 = 62;     // output columns per strip
-constexpr int kRowW2 = 66;   // staged columns per row: 65 used, even for 8-byte copies
-
-__device__ __forceinline__ void cp_async8_partial(float* smem, const float* gmem, int bytes) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
-}
-
-template <int NF>
-struct Stream2 {
-  float* ring;
-  const float* const* fields;
-  int x0, y0, z0, nlayers, total, rows;
-  const LevelGeo* g;
-
-  __device__ __forceinline__ void issue(int s, int lane) {
-    if (s < total) {
-      const int li = s / rows, r = s - li * rows;
-      const int kk = z0 - 1 + li, y = y0 - 1 + r;
-      const int slot = s & (kRing - 1);
-      const int col = x0 - 2 + 2 * lane, colx = x0 + 62;
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        const int z = kk + c;
-        const bool row_ok = y >= 0 && y < g->ny && z >= 0 && z < g->nz;
-        const bool ok = row_ok && col >= 0 && col < g->nx;
-        const int bytes = ok ? (col + 1 < g->nx ? 8 : 4) : 0;
-        const long long n = ok ? (long long)col + (long long)y * g->px + (long long)z * g->plane : 0;
-        const bool okx = row_ok && colx < g->nx;
-        const long long nx_ = okx ? (long long)colx + (long long)y * g->px + (long long)z * g->plane : 0;
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-          float* row = ring + ((slot * NF + f) * 2 + c) * kRowW2;
-          cp_async8_partial(row + 2 * lane, fields[f] + n, bytes);
-          if (lane == 31) cp_async4(row + 64, fields[f] + nx_, okx);
-        }
-      }
-    }
-    cp_async_commit();
-  }
-  __device__ __forceinline__ float at(int s, int f, int c, int col) const {
-    return ring[(((s & (kRing - 1)) * NF + f) * 2 + c) * kRowW2 + col];
-  }
-  __device__ __forceinline__ float2 at2(int s, int f, int c, int col) const {  // col even
-    return *reinterpret_cast<const float2*>(ring + (((s & (kRing - 1)) * NF + f) * 2 + c) * kRowW2 + col);
-  }
-};
-
-template <bool FINEST, int EPI, bool ISO>
-__global__ void __launch_bounds__(kWarps * 32) mech_x2_kernel(MechKT<float> k) {
-  constexpr int NF = 3 + (FINEST ? 0 : 2);  // u, then Ke, Ge on coarse levels (finest: moduli from gpm)
-  extern __shared__ __align__(16) unsigned char x2_smem[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  float* ring = reinterpret_cast<float*>(x2_smem) + (size_t)wib * (kRing * NF * 2 * kRowW2 + (kWY - 1) * 3 * 64);
-  float2* zc = reinterpret_cast<float2*>(ring + kRing * NF * 2 * kRowW2);  // [row][comp][lane]
-  const SFt<F2> s = make_sf<F2>(k.g);
-  const float wgs = ISO ? (float)k.g.wg * (float)(1.0 / k.g.hx) * (float)(1.0 / k.g.hx) : (float)k.g.wg;
-  double red0 = 0.0, red1 = 0.0, red2 = 0.0;
-  const long long nwarps_total = (long long)gridDim.x * kWarps;
-  const float* fptr[NF];
-#pragma unroll
-  for (int f = 0; f < NF; ++f) fptr[f] = k.fields[f];
-  const long long N = k.g.n;
-
-  for (long long strip = (long long)blockIdx.x * kWarps + wib; strip < k.sg.nstrips; strip += nwarps_total) {
-    const int sx = (int)(strip % k.sg.tx);
-    const long long rest = strip / k.sg.tx;
-    const int sy = (int)(rest % k.sg.ty);
-    const int sz = (int)(rest / k.sg.ty);
-    const int wy = k.sg.wy, rows = wy + 1;
-    const int x0 = sx * kOX2, y0 = sy * (wy - 1), z0 = sz * k.sg.cz;
-    const int c0 = x0 - 2 + 2 * lane, c1 = c0 + 1;
-    const int zend = min(z0 + k.sg.cz - 1, k.g.nz - 1);
-    Stream2<NF> st{ring, fptr, x0, y0, z0, zend - z0 + 2, 0, rows, &k.g};
-    st.total = st.nlayers * rows;
-    st.issue(0, lane);
-    st.issue(1, lane);
-    F2 yp[2][3];
-    for (int si = 0; si < st.total; ++si) {
-      st.issue(si + 2, lane);
-      cp_async_wait2();
-      __syncwarp();
-      const int li = si / rows, r = si - li * rows;
-      const int kk = z0 - 1 + li;
-      if (r == 0) {
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-#pragma unroll
-          for (int m = 0; m < 3; ++m) yp[c][m] = F2(0.0f);
-        __syncwarp();
-        continue;
-      }
-      const int rr = r - 1, ey = y0 - 1 + rr;
-      const bool out_row = rr >= 1 && kk >= z0 && lane >= 1 && ey < k.g.ny;
-      if (EPI == EPI_RESIDUAL && out_row && c0 < k.g.nx) {
-        const long long n = (long long)c0 + (long long)ey * k.g.px + (long long)kk * k.g.plane;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(k.fu + n + m * N));
-          if (k.invM) asm volatile("prefetch.global.L2 [%0];" ::"l"(k.invM + n + m * N));
-        }
-      }
-      // ---- elements E0 (x = c0) and E1 (x = c1) of row ey, layer kk
-      const bool row_valid = ey >= 0 && ey <= k.g.ny - 2 && kk >= 0 && kk <= k.g.nz - 2;
-      const bool v0 = row_valid && c0 >= 0 && c0 <= k.g.nx - 2;
-      const bool v1 = row_valid && c1 >= 0 && c1 <= k.g.nx - 2;
-      F2 f[3][8];
-      if (v0 || v1) {
-        F2 Kw[8], Gw[8];
-        const long long e0 = (long long)c0 + (long long)ey * k.g.px + (long long)kk * k.g.plane;
-        if (FINEST) {
-#pragma unroll
-          for (int g = 0; g < 8; ++g) {
-            Kw[g].v = *reinterpret_cast<const float2*>(k.gpm + (long long)g * N + e0);
-            Gw[g].v = *reinterpret_cast<const float2*>(k.gpm + (long long)(8 + g) * N + e0);
-          }
-        } else {
-          const float2 ke = st.at2(si - 1, 3, 0, 2 * lane), ge = st.at2(si - 1, 4, 0, 2 * lane);
-          const F2 K(ke.x * wgs, ke.y * wgs), G(ge.x * wgs, ge.y * wgs);
-#pragma unroll
-          for (int g = 0; g < 8; ++g) {
-            Kw[g] = K;
-            Gw[g] = G;
-          }
-        }
-        F2 u[3][8];
-#pragma unroll
-        for (int n = 0; n < 8; ++n) {
-          const int a = n & 1, b = (n >> 1) & 1, c = n >> 2;
-          const int srow = b ? si : si - 1;
-#pragma unroll
-          for (int m = 0; m < 3; ++m) {
-            if (a == 0) {
-              u[m][n].v = st.at2(srow, m, c, 2 * lane);
-            } else {
-              u[m][n].v = make_float2(st.at(srow, m, c, 2 * lane + 1), st.at(srow, m, c, 2 * lane + 2));
-            }
-          }
-        }
-        mech_element<ISO>(u, Kw, Gw, s, f);
-#pragma unroll
-        for (int m = 0; m < 3; ++m)
-#pragma unroll
-          for (int n = 0; n < 8; ++n) {
-            if (!v0) f[m][n].v.x = 0.f;
-            if (!v1) f[m][n].v.y = 0.f;
-          }
-      } else {
-#pragma unroll
-        for (int m = 0; m < 3; ++m)
-#pragma unroll
-          for (int n = 0; n < 8; ++n) f[m][n] = F2(0.0f);
-      }
-      // ---- nodes (c0, c1) of each face: (E0.a0 + left lane's E1.a1, E0.a1 + E1.a0)
-      F2 X[2][2][3];  // [b][c][m]
-#pragma unroll
-      for (int c = 0; c < 2; ++c)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-          for (int m = 0; m < 3; ++m) {
-            const F2 lo = f[m][2 * b + 4 * c], hi = f[m][1 + 2 * b + 4 * c];
-            const float left = __shfl_up_sync(kFull, hi.v.y, 1);
-            X[b][c][m] = F2(lo.v.x + (lane > 0 ? left : 0.f), hi.v.x + lo.v.y);
-          }
-      if (rr >= 1) {
-        const int orow = rr - 1;
-        F2 tot[3];
-#pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          float2* zp = zc + (orow * 3 + m) * 32 + lane;
-          F2 zv;
-          zv.v = *zp;
-          tot[m] = zv + yp[0][m] + X[0][0][m];
-          *zp = (yp[1][m] + X[0][1][m]).v;
-        }
-        if (out_row) {
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int x = c0 + h;
-            if (x >= k.g.nx) continue;
-            const long long n = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
-            float tv[3];
-#pragma unroll
-            for (int m = 0; m < 3; ++m) tv[m] = h ? tot[m].v.y : tot[m].v.x;
-            if (EPI == EPI_PLAIN) {
-#pragma unroll
-              for (int m = 0; m < 3; ++m) k.out[n + m * N] = tv[m];
-            } else if (EPI == EPI_RESIDUAL) {
-              const BcFlags bc = bc_flags(k.g, x, ey, kk);
-              const bool fix[3] = {bc.c0, bc.c1, bc.c2};
-#pragma unroll
-              for (int m = 0; m < 3; ++m) {
-                const float fv = k.fu[n + m * N];
-                red0 = fma((double)fv, (double)fv, red0);
-                const float rv = fix[m] ? 0.f : fv - tv[m];
-                k.out[n + m * N] = rv;
-                if (k.invM) red1 = fma((double)rv, (double)(rv * k.invM[n + m * N]), red1);
-                red2 = fma((double)rv, (double)rv, red2);
-              }
-            } else if (EPI == EPI_PCG) {
-#pragma unroll
-              for (int m = 0; m < 3; ++m) {
-                k.out[n + m * N] = tv[m];
-                red0 = fma((double)st.at(si - 1, m, 0, 2 * lane + h), (double)tv[m], red0);
-              }
-            } else if (EPI == EPI_FAS) {
-#pragma unroll
-              for (int m = 0; m < 3; ++m)
-                k.out[n + m * N] = tv[m] + full_weight(k.gf, k.rf + (long long)m * k.gf.n, 2 * x, 2 * ey, 2 * kk);
-            }
-          }
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 2; ++c)
-#pragma unroll
-        for (int m = 0; m < 3; ++m) yp[c][m] = X[1][c][m];
-      __syncwarp();
-    }
-  }
-  if (EPI == EPI_RESIDUAL || EPI == EPI_PCG) {
-    double v[3] = {red0, red1, red2};
-    grid_reduce<3>(v, k.red);
-  }
-}
-
-template <bool F, int E>
-static int run_x2(hpc_ctx* c, const MechKT<float>& k) {
-  constexpr int NF = 3 + (F ? 0 : 2);
-  const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW2 + (kWY - 1) * 3 * 64) * sizeof(float);
-  if (iso(k.g)) return launch_strips(c, mech_x2_kernel<F, E, true>, k, smem, HPC_KC_NONE, kOX2);
-  return launch_strips(c, mech_x2_kernel<F, E, false>, k, smem, HPC_KC_NONE, kOX2);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -574,24 +574,30 @@ static int f32_material(hpc_ctx* c) {
 }
 
 // pcg_u (mechanical_pcg.cpp:223-330) on the FP32 mirror, homogeneous Dirichlet values.
-static int pcg_u32(hpc_ctx* c, int l, double small_k, int nb) {
+// u_zero: the unknown is known to be zero (the finest pre-smoother of the correction), so the first
+// residual is f itself and needs no operator apply.
+static int pcg_u32(hpc_ctx* c, int l, double small_k, int nb, bool u_zero = false) {
   if (nb > kMaxRelax) return arg_fail("nb_relax too large");
   LevelF32& F = c->F32[l];
   int rc;
-  if ((rc = launch_bc_zero_f32(c, l, F.u))) return rc;
   MechCall32 m{};
   m.level = l;
   m.finest = is_finest(c, l);
-  m.epi = EPI_RESIDUAL;
-  m.src = F.u;
-  m.out = F.ru;
-  m.small_k = small_k;
-  m.fu = F.fu;
-  m.invM = F.invM;
-  m.s_out0 = -1;
-  m.s_out1 = slot_rz(0);
-  m.s_out2 = -1;
-  if ((rc = launch_mech_f32(c, m))) return rc;
+  if (u_zero) {
+    if ((rc = launch_residual_zero_f32(c, l, slot_rz(0)))) return rc;
+  } else {
+    if ((rc = launch_bc_zero_f32(c, l, F.u))) return rc;
+    m.epi = EPI_RESIDUAL;
+    m.src = F.u;
+    m.out = F.ru;
+    m.small_k = small_k;
+    m.fu = F.fu;
+    m.invM = F.invM;
+    m.s_out0 = -1;
+    m.s_out1 = slot_rz(0);
+    m.s_out2 = -1;
+    if ((rc = launch_mech_f32(c, m))) return rc;
+  }
   for (int it = 0; it < nb; ++it) {
     if ((rc = launch_dir_update_f32(c, l, it == 0, slot_rz(it), slot_rz(it - 1)))) return rc;
     MechCall32 q{};
@@ -727,7 +733,7 @@ static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double
       if (L == 0) {
         if ((rc = cycle_u32(c, 0, mg, small_k))) return rc;
       } else {
-        if ((rc = pcg_u32(c, L, small_k, mg.nu1))) return rc;
+        if ((rc = pcg_u32(c, L, small_k, mg.nu1, true))) return rc;
         if ((rc = run_graphed(c, c->g32, mg, small_k, 0.0, k > 0,
                               [&] { return coarse_part_u32(c, L, mg, small_k); })))
           return rc;
@@ -903,7 +909,6 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   c->choice_quirk = 1;
   c->use_graphs = 1;
   c->fused_coarsest = 1;
-  c->f32_pairs = 1;
   c->timing_class = HPC_KC_NONE;
   HostLevel lv[kMaxLevels];
   host_geometry(*geo, c->box, lv);
@@ -1057,12 +1062,6 @@ int hpc_level_dims(hpc_ctx* c, int level, int* n3, double* h3) {
 int hpc_sync(hpc_ctx* c) {
   if (!c) return arg_fail("null context");
   HPC_CUDA(cudaStreamSynchronize(c->stream));
-  return HPC_OK;
-}
-
-int hpc_set_f32_pairs(hpc_ctx* c, int on) {
-  if (!c) return arg_fail("null context");
-  c->f32_pairs = on != 0;
   return HPC_OK;
 }
 

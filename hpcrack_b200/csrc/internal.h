@@ -110,7 +110,6 @@ struct hpc_ctx {
   int autotune;  // measure strip shapes on first use (hpc_set_autotune)
   int fused_coarsest;  // coarse-level pcg_u in one block when the level fits (hpc_set_fused_coarsest)
   int gpm_active;      // finest applies read F[maxlevel].gpm (set while a mechanical solve runs)
-  int f32_pairs;       // FP32 operator with two elements per lane (hpc_set_f32_pairs)
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
@@ -211,6 +210,8 @@ int launch_mech_update_f32(hpc_ctx* c, int level, int s_num, int s_den, int s_rz
 // FP32 mirror: p = r M^-1 + beta p (beta from scal, 0 if first)
 int launch_dir_update_f32(hpc_ctx* c, int level, bool first, int s_rz, int s_rz_prev);
 int launch_bc_zero_f32(hpc_ctx* c, int level, float* v);  // zero the Dirichlet rows of a 3n vector
+// FP32 mirror: r = f (Dirichlet rows zero) and (r, M^-1 r) for a correction whose unknown is zero
+int launch_residual_zero_f32(hpc_ctx* c, int level, int s_rz);
 int launch_inject_u_f32(hpc_ctx* c, int lf);             // u_c = u_f(2i), Dirichlet rows 0, uold_c = u_c
 int launch_prolong_f32(hpc_ctx* c, int lf);              // u_f += P(u_c - uold_c), Dirichlet rows 0
 int launch_to_f32(hpc_ctx* c, const double* src, float* dst, long long n);

@@ -920,3 +920,40 @@ int launch_prolong_f32(hpc_ctx* c, int lf) {
   return HPC_OK;
 }
 }  // namespace hpc
+
+namespace hpc {
+// The residual of the correction problem when its unknown is still zero: r = f with Dirichlet rows
+// zero, (r, M^-1 r) into a slot - the first residual of the precision form's finest pre-smoother,
+// without an operator apply.
+__global__ void residual_zero_f32_kernel(LevelGeo g, const float* f, const float* invM, float* r, RedTarget red) {
+  double rz = 0.0;
+  FOR_NODES(g) {
+    const long long n = nidx(g, i, j, kz);
+    bool fix[3] = {false, false, false};
+    if (g.bz[kz]) {
+      const BcFlags bc = bc_flags(g, i, j, kz);
+      fix[0] = bc.c0;
+      fix[1] = bc.c1;
+      fix[2] = bc.c2;
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const long long o = n + (long long)m * g.n;
+      const float rv = fix[m] ? 0.f : f[o];
+      r[o] = rv;
+      rz = fma((double)rv, (double)(rv * invM[o]), rz);
+    }
+  }
+  double v[1] = {rz};
+  grid_reduce<1>(v, red);
+}
+
+int launch_residual_zero_f32(hpc_ctx* c, int level, int s_rz) {
+  const LevelGeo& g = c->L[level];
+  const LevelF32& F = c->F32[level];
+  residual_zero_f32_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, F.fu, F.invM, F.ru,
+                                                                       make_red(c, s_rz, -1, -1));
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+}  // namespace hpc

@@ -147,10 +147,6 @@ class Hierarchy:
         self._c("hpc_download_choice", level, a.ctypes.data_as(C.POINTER(C.c_int16)))
         return a
 
-    def set_f32_pairs(self, on: bool):
-        """Precision form's FP32 operator with two elements per lane (default) or one."""
-        self._c("hpc_set_f32_pairs", int(bool(on)))
-
     def set_fused_coarsest(self, on: bool):
         """Coarsest-level pcg_u in one thread block (default) or as per-iteration kernels."""
         self._c("hpc_set_fused_coarsest", int(bool(on)))

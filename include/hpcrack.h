@@ -127,9 +127,6 @@ int hpc_tuned_shapes(int* out5, int cap, int* count);
  * shared memory (up to about 10^3 nodes); 0 uses the per-iteration kernels.  The two differ only in
  * the order of the same sums. */
 int hpc_set_fused_coarsest(hpc_ctx* ctx, int on);
-/* No counterpart in the reference: 1 (default) runs the precision form's single-precision operator
- * with two x-adjacent elements per lane in packed FP32x2 arithmetic; 0 one element per lane. */
-int hpc_set_f32_pairs(hpc_ctx* ctx, int on);
 /* Kernels launched by this context since the last reset (instrumentation for benchmarks). */
 int hpc_launch_count(hpc_ctx* ctx, long long* count, int reset);
 /* The context's CUDA stream (cudaStream_t), for callers that time on it. */

@@ -69,23 +69,3 @@ def test_fcg_increments_match_fas():
         for a, b in zip(fb, fa):
             assert abs(a[1] - b[1]) <= 1e-6 * abs(b[1])  # reaction force
 
-
-@pytest.mark.parametrize("name", ["small33", "mid129"])
-def test_paired_fp32_operator_matches_single(name):
-    """The precision form with the paired-element FP32x2 operator and with the one-element FP32
-    operator: both meet the stopping test, with V-cycle counts within 2 and solutions within the
-    accuracy the test allows."""
-    w = ms.make_workload(name)
-    L = w.maxlevel
-    res = []
-    for pairs in (True, False):
-        h = _fresh(w)
-        h.set_f32_pairs(pairs)
-        cy, _, fn = h.u_entire_fcg(w.mg_u, w.small_k, 1.0, 0, 0.0, mech_tol=1e-16, mixed=True)
-        r2 = h.initial_residual_u(L, w.small_k)
-        res.append((cy, r2 / fn, h.get(U, L)))
-        h.close()
-    (c1, q1, u1), (c2, q2, u2) = res
-    assert q1 <= 1e-15 and q2 <= 1e-15
-    assert abs(c1 - c2) <= 2, (c1, c2)
-    assert rel(u1, u2) < (1e-6 if not w.crack else 1e-4)
