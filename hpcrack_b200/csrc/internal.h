@@ -159,25 +159,21 @@ double* vector_field(hpc_ctx* c, int field, int level);  // nullptr if not a vec
 int read_scalars(hpc_ctx* c, int first, int count, double* out);  // sync + D2H of scalar slots
 int write_scalar(hpc_ctx* c, int slot, double v);
 
-// ---------------------------------------------------------------- kernel launchers (kernels.cu)
-// Element operators.  `src` is a 3n (mech) or n (pf) vector on level L.
+// ---------------------------------------------------------------- kernel launchers
+// Element operators (element_kernels.cu).  `src` is a 3n (mech) or n (pf) vector on level L.
 enum MechEpi { EPI_PLAIN = 0, EPI_RESIDUAL = 1, EPI_PCG = 2, EPI_FAS = 3, EPI_REACTION = 4 };
 
 struct MechCall {
   int level;
   bool finest;
   int epi;
-  const double* src;  // u (PLAIN / RESIDUAL / FAS / REACTION) or p_old (PCG)
+  const double* src;  // u (PLAIN / RESIDUAL / FAS / REACTION) or p (PCG)
   double* out;        // Fi (PLAIN), r (RESIDUAL), w (PCG), fc (FAS), fu (REACTION: BC slots only)
   double small_k;
   // RESIDUAL: r = fu - K u, zero at Dirichlet nodes; optionally fu[bc] = (K u)[bc] and f_norm.
   double* fu;
   bool set_fnorm;     // t == 0 on the finest level (mechanical_pcg.cpp:252-258)
-  const double* invM; // inverse diagonal; RESIDUAL: rz = sum r^2 invM ; PCG: z = r invM
-  // PCG: p_new = r invM + beta p_old with beta = scal[s_rz]/scal[s_rz_prev] (0 if first)
-  const double* r;
-  double* p_new;
-  int s_rz, s_rz_prev, first;
+  const double* invM; // RESIDUAL: inverse diagonal for rz = sum r^2 invM (null: no rz)
   // FAS: fc = K_c u_c + full-weighting(rf)
   const double* rf;
   int fine_level;
@@ -224,10 +220,7 @@ struct PfCall {
   double* out;
   double lc;
   const double* fd;     // RESIDUAL: R = fd - A d
-  const double* invM;   // inverse diagonal (PCG, and rz in RESIDUAL)
-  const double* r;
-  double* p_new;
-  int s_rz, s_rz_prev, first;
+  const double* invM;   // RESIDUAL: inverse diagonal for rz (null: no rz)
   const double* rf;
   int fine_level;
   int s_out0, s_out1, s_out2;
@@ -235,7 +228,7 @@ struct PfCall {
 int launch_pf(hpc_ctx* c, const PfCall& p);
 int launch_pf_diag(hpc_ctx* c, int level, double lc, double* out);
 
-// Vector kernels.
+// Vector kernels (vector_kernels.cu).
 // Mechanical CG update: alpha = scal[s_rz]/scal[s_pw]; u += alpha p; r -= alpha w; r = 0 on Dirichlet
 // nodes; scal[s_rz_next] = sum r^2/preM; scal[s_rn] = sum r^2.
 int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
