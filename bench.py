@@ -168,6 +168,9 @@ def run_profile_cycles(args, local):
     hier = load_specimen(w, local)
     K = args.profile_cycles
     mg_u = tuple(w.mg_u[:4]) + (K,)
+    if args.mech_solver != "fas" and not args.mg_u:
+        from hpcrack_b200.solver import precision_mg
+        mg_u = precision_mg(w.maxlevel, w.element_nb, K)
     mg_d = tuple(w.mg_d[:4]) + (K,)
     launches0 = hier.launch_count()
     outs = [hier.step(t, mg_u, mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du, dU_factor=w.du_factor,
