@@ -1010,6 +1010,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
 int hpc_destroy(hpc_ctx* c) {
   if (!c) return HPC_OK;
   cudaSetDevice(c->device);
+  vtk_release(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
     LevelFields& F = c->F[l];

@@ -130,6 +130,16 @@ struct hpc_ctx {
   struct Fcg {
     double *x, *r, *rp, *f, *p;  // iterate, residual, previous residual, right-hand side (fu saved), direction
   } fcg;
+  // VTK output (hpc_vtk_write): base64 characters of one field on the device and in pinned host
+  // memory, a copy stream, and the host thread writing the files (allocated on first use)
+  struct Vtk {
+    char* dev;
+    char* host;
+    size_t cap;
+    cudaStream_t stream;
+    cudaEvent_t packed, copied;
+    void* job;
+  } vtk;
 };
 
 namespace hpc {
@@ -158,6 +168,8 @@ double* scalar_field(hpc_ctx* c, int field, int level);  // nullptr if not a sca
 double* vector_field(hpc_ctx* c, int field, int level);  // nullptr if not a vector field
 int read_scalars(hpc_ctx* c, int first, int count, double* out);  // sync + D2H of scalar slots
 int write_scalar(hpc_ctx* c, int slot, double v);
+// Waits for a VTK write in flight and frees the VTK buffers (vtk_output.cu); returns that write's status.
+int vtk_release(hpc_ctx* c);
 
 // ---------------------------------------------------------------- kernel launchers
 // Element operators (element_kernels.cu).  `src` is a 3n (mech) or n (pf) vector on level L.

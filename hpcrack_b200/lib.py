@@ -16,7 +16,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "hpcrack.h")
 
 HPC_OK = 0
 STATUS = {0: "HPC_OK", 1: "HPC_ERR_ARG", 2: "HPC_ERR_CUDA", 3: "HPC_ERR_NOMEM", 4: "HPC_ERR_DIVZERO",
-          5: "HPC_ERR_INPUT", 6: "HPC_ERR_NODEVICE"}
+          5: "HPC_ERR_INPUT", 6: "HPC_ERR_NODEVICE", 7: "HPC_ERR_IO"}
 
 
 class HpcError(RuntimeError):
@@ -72,6 +72,8 @@ SIGNATURES = {
     "hpc_get_state": [_ctx, _dp],
     "hpc_set_state": [_ctx, _dp],
     "hpc_checkpoint_begin": [_ctx, _i],
+    "hpc_vtk_write": [_ctx, C.c_char_p, _i, _i, _d, C.c_char_p, C.c_char_p, _i],
+    "hpc_vtk_wait": [_ctx],
     "hpc_checkpoint_wait": [_ctx, _ip, C.POINTER(_dp), _dp],
     "hpc_checkpoint_restore": [_ctx, _dp, _dp, _dp, _dp, _dp, _dp, _dp],
     "hpc_internal_force": [_ctx, _i, _i, _i, _d],

@@ -1,7 +1,8 @@
 // Device-resident staggered loop: a drop-in for crack_propagation (crack_propagation.cpp:28-123)
 // with the same signature, constants, load schedule, stop test, console lines, F_U.dat format,
 // history dumps and VTK output.  u, d and H live on the device for the whole run; each increment
-// is one hpc_step call, and host copies are made only for the dumps the configuration asks for.
+// is one hpc_step call, host copies are made only for the dumps the configuration asks for, and the
+// VTK files of d are encoded on the device and written by a host thread while the loop goes on.
 #include <fstream>
 #include <iomanip>
 #include <iostream>
@@ -69,7 +70,9 @@ void crack_propagation(Stack* U, const mgdouble& bulK, const mgdouble& G, const 
       write_vector_3D(fetch(HPC_D, 0), "d", myid, t);
     }
     const double dmax = out[3];
-    if (t == 0 || dmax >= 0.98) write_total_de(U, fetch(HPC_D, 0), M, "S", "d", "d", L, myid, nbprocs, t);
+    // write_total_de(U, d, M, "S", "d", "d", L, myid, nbprocs, t) from the device: the same files,
+    // written while the next increment runs
+    if (t == 0 || dmax >= 0.98) check(hpc_vtk_write(c, "S", HPC_D, L, 1.0, "d", "d", t), "hpc_vtk_write");
     const double Ut = s6[3], delta_U = s6[4], F = out[1];
     if (myid == 0) {
       F_U << "T= " << t << ",U= " << std::setprecision(10) << Ut << " ,Fw= " << std::setprecision(10) << F
@@ -78,5 +81,6 @@ void crack_propagation(Stack* U, const mgdouble& bulK, const mgdouble& G, const 
     if (F < 0.5) break;
   }
   F_U.close();
+  check(hpc_vtk_wait(c), "hpc_vtk_wait");
   hpc_shim_release_all();
 }

@@ -178,6 +178,18 @@ class Hierarchy:
     # ------------------------------------------------------------ checkpoint / restart
     CHECKPOINT_FIELDS = ("u", "v", "w", "H", "d", "d_old")
 
+    def vtk_write(self, option: str, field: int, level: int, filename: str, field_name: str, t: int,
+                  scale: float = 1.0):
+        """The reference's write_total_de ("S"), write_total_u ("V", values times `scale`) or
+        write_total_H ("C") of one field of one level: Output/<filename>_l_<level>_t_<t>_Proc_0.vti
+        and the .pvti index, relative to the working directory.  Asynchronous: vtk_wait() (or the
+        next vtk_write) waits for the files."""
+        self._c("hpc_vtk_write", option.encode(), int(field), int(level), float(scale), filename.encode(),
+                field_name.encode(), int(t))
+
+    def vtk_wait(self):
+        self._c("hpc_vtk_wait")
+
     def checkpoint_begin(self, t: int):
         """Snapshot the loop state on the device and start its copy to host memory (asynchronous)."""
         self._c("hpc_checkpoint_begin", int(t))

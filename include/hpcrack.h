@@ -44,7 +44,8 @@ enum hpc_status {
   HPC_ERR_DIVZERO = 4,    /* zero diagonal entry: the reference throws "Division by zero in grid /=
                              operation" (include/grid.h:182-190) */
   HPC_ERR_INPUT = 5,      /* gray level outside the material table, malformed input */
-  HPC_ERR_NODEVICE = 6    /* no CUDA device */
+  HPC_ERR_NODEVICE = 6,   /* no CUDA device */
+  HPC_ERR_IO = 7          /* an output file could not be opened or written */
 };
 
 /* Field ids (the reference's containers: crack_propagation.cpp:40-45, mechanical_displacement.cpp:
@@ -169,6 +170,26 @@ int hpc_checkpoint_wait(hpc_ctx* ctx, int* t, const double** fields, double* sta
  * the fields) and the loop state; the next hpc_step continues as the uninterrupted run would. */
 int hpc_checkpoint_restore(hpc_ctx* ctx, const double* u, const double* v, const double* w, const double* H,
                            const double* d, const double* d_old, const double* state6);
+
+/* ---------------- VTK output ---------------- */
+/* write_total_de / write_total_u / write_total_H (vtk_output.cpp:420-469) of one rank: the .vti
+ * piece (Float32 values, base64, XML ImageData) and the .pvti index of one field of one level,
+ * byte-identical to the reference's files.  option "S": scalar point data (a scalar field), "V":
+ * vector point data (a vector field, every value multiplied by `scale` first, as write_vector does
+ * with u_proportion), "C": cell data of the element slots (write_celltdata_H).  Paths follow
+ * open_file / write_pvtk (vtk_output.cpp:26-35, :362-367): Output/<filename>_l_<level>_t_<t>_Proc_0.vti
+ * and Output/<filename>_l_<level>_t_<t>.pvti unless filename contains ".vti" / ".pvti"; the Output
+ * folder must exist.  The field is converted and encoded on the device on the context's stream,
+ * copied to pinned host memory on a copy stream and written by a host thread, so the call returns
+ * at once and later work on the context overlaps the copy and the writes; the first call allocates
+ * the character buffers (16 bytes per node for "V", 16/3 for "S"), on the device and in pinned host
+ * memory.  One write is in flight per context: a second call first waits for the previous one.
+ * The reference's combined "VS" writer (write_total_Eu) is not offered: its file lacks the second
+ * DataArray's opening tag. */
+int hpc_vtk_write(hpc_ctx* ctx, const char* option, int field, int level, double scale, const char* filename,
+                  const char* field_name, int t);
+/* Waits for the write in flight; returns its status (HPC_ERR_IO if a file could not be written). */
+int hpc_vtk_wait(hpc_ctx* ctx);
 
 /* ---------------- operators ---------------- */
 /* Internal_Force: dst = K(d) src on one level (mechanical_pcg.cpp:174-191). */

@@ -391,6 +391,8 @@ class RefOracle(_Base):
             "last_output": (C.c_char_p, []),
             "write_vector_3d": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]),
             "read_vector_3d": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_int]),
+            "write_vtk": (C.c_int, [vp, C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_char_p, C.c_int,
+                                    C.c_double, C.c_char_p]),
         }
 
     def _create(self, maxlevel, enb, x0, roi):
@@ -457,3 +459,10 @@ class RefOracle(_Base):
         """The reference's read_vector_3D (write_read_history.cpp:55-86) of `path` into one grid."""
         if self.lib.ref_read_vector_3d(self.h, field, level, comp, path.encode(), t) != 0:
             raise ValueError("bad field")
+
+    def write_vtk(self, option, field, level, filename, field_name, t, workdir, u_proportion=1.0):
+        """The reference's write_total_de ("S"), write_total_u ("V") or write_total_H ("C")
+        (vtk_output.cpp:420-469), one rank, writing below `workdir`/Output."""
+        if self.lib.ref_write_vtk(self.h, option.encode(), field, level, filename.encode(), field_name.encode(),
+                                  t, u_proportion, workdir.encode()) != 0:
+            raise ValueError("bad option, field or workdir")

@@ -45,6 +45,7 @@
 #include "image_input.h"
 #include "pcg_utilities.h"
 #include "write_read_history.h"
+#include "vtk_output.h"
 
 namespace {
 
@@ -621,6 +622,36 @@ int ref_read_vector_3d(void* h, int field, int level, int comp, const char* path
   if (!g) return -1;
   captured([&] { read_vector_3D(*g, std::string(path), 0, t); });
   return 0;
+}
+
+// write_total_de ("S"), write_total_u ("V", scaled by u_proportion) or write_total_H ("C") of
+// vtk_output.cpp:420-469 for one rank, run in `workdir` (the reference writes below ./Output).
+int ref_write_vtk(void* h, const char* option, int field, int level, const char* filename, const char* field_name,
+                  int t, double u_proportion, const char* workdir) {
+  RefCtx* c = (RefCtx*)h;
+  char cwd[4096];
+  if (!getcwd(cwd, sizeof cwd) || chdir(workdir) != 0) return -1;
+  int rc = 0;
+  const std::string opt(option);
+  captured([&] {
+    if (opt == "S") {
+      griddouble* g = grid_of(c, field, level, 0);
+      if (g) write_total_de(&c->U, *g, c->M, opt, filename, field_name, level, 0, 1, t);
+      else rc = -1;
+    } else if (opt == "V") {
+      mgvecdouble* v = vector_field(c, field);
+      if (v) write_total_u(&c->U, v->getLevel(level), c->M, level, 0, 1, filename, field_name, t, u_proportion);
+      else rc = -1;
+    } else if (opt == "C") {
+      griddouble* g = grid_of(c, field, level, 0);
+      if (g) write_total_H(&c->U, *g, c->M, opt, filename, field_name, level, 0, 1, t);
+      else rc = -1;
+    } else {
+      rc = -1;
+    }
+  });
+  if (chdir(cwd) != 0) return -1;
+  return rc;
 }
 
 }  // extern "C"

@@ -67,3 +67,62 @@ def load_workload(impls, w: ms.Workload):
             impl.set(H, w.maxlevel, Hc)
             impl.set(D, w.maxlevel, dc)
             impl.voigt_all_level(H)
+
+
+def vtk_expected(option, values, dims, origin, spacing, filename, field_name, level, t, scale=1.0):
+    """The .vti and .pvti bytes the reference's write_total_de ("S"), write_total_u ("V") and
+    write_total_H ("C") produce for one rank (vtk_output.cpp:26-469), built independently from the
+    file format: XML text, Float32 values x fastest (vector components interleaved, element slots
+    for cell data), base64 of the 4-byte length header and of the values as two separate blocks.
+    `values`: dense x-fastest doubles, shape (n,) or (3, n) for "V"."""
+    import base64
+
+    nx, ny, nz = dims
+    ii, jj, kk = nx - 1, ny - 1, nz - 1
+    if option == "V":
+        v = np.asarray(values, dtype=np.float64).reshape(3, -1)
+        data = (scale * v).T.astype(np.float32).ravel()
+    elif option == "C":
+        a = np.asarray(values, dtype=np.float64).reshape(nz, ny, nx)[:kk, :jj, :ii]
+        data = a.astype(np.float32).ravel()
+    else:
+        data = np.asarray(values, dtype=np.float64).astype(np.float32).ravel()
+    raw = data.astype("<f4").tobytes()
+    hdr = base64.b64encode(np.uint32(len(raw)).astype("<u4").tobytes())
+    x0, y0, z0 = origin
+    hx, hy, hz = spacing
+    head = ('<?xml version="1.0"?>\n'
+            '<VTKFile type="ImageData" version="0.1" byte_order="LittleEndian">\n'
+            f'<ImageData WholeExtent="0 {ii} 0 {jj} 0 {kk} " \t\t\t\tOrigin="{x0:f} {y0:f} {z0:f}" '
+            f'Spacing="{hx:f} {hy:f} {hz:f}">\n'
+            f'<Piece Extent="0 {ii} 0 {jj} 0 {kk}" >\n')
+    ncomp = 3 if option == "V" else 1
+    array = f'<DataArray Name="{field_name}" type="Float32" NumberOfComponents="{ncomp}" format="binary">\n'
+    if option == "C":
+        head += f'<PointData></PointData>\n<CellData Scalar = "{field_name}">\n' + array
+        tail = "\n</DataArray>\n</CellData>\n"
+    else:
+        head += f'<PointData {"Vectors" if option == "V" else "Scalars"}="{field_name}">\n' + array
+        tail = "\n</DataArray>\n</PointData>\n<CellData></CellData>\n"
+    tail += "</Piece>\n</ImageData>\n</VTKFile>"
+    vti = head.encode() + hdr + base64.b64encode(raw) + tail.encode()
+    p = ('<?xml version="1.0"?>\n'
+         '<VTKFile type="PImageData" version="0.1" byte_order="LittleEndian">\n'
+         f'<PImageData WholeExtent="0 {ii} 0 {jj} 0 {kk} " \t\t\t\tGhostLevel="0" Origin="{x0:f} {y0:f} {z0:f}" '
+         f'Spacing="{hx:f} {hy:f} {hz:f}">\n')
+    parray = f'<PDataArray Name="{field_name}" type="Float32" NumberOfComponents="{ncomp}"/>\n'
+    if option == "C":
+        p += f'<PPointData></PPointData>\n<PCellData Scalar = "{field_name}">\n' + parray + "</PCellData>\n"
+    else:
+        p += f'<PPointData {"Vectors" if option == "V" else "Scalars"}="{field_name}">\n' + parray
+        p += "</PPointData>\n<PCellData></PCellData>\n"
+    p += (f'<Piece Extent="0 {ii} 0 {jj} 0 {kk}" Source="{filename}_l_{level}_t_{t}_Proc_0.vti"/>\n'
+          "</PImageData>\n</VTKFile>\n")
+    return vti, p.encode()
+
+
+def vtk_paths(workdir, filename, level, t):
+    import os
+
+    return (os.path.join(workdir, "Output", f"{filename}_l_{level}_t_{t}_Proc_0.vti"),
+            os.path.join(workdir, "Output", f"{filename}_l_{level}_t_{t}.pvti"))
