@@ -62,6 +62,9 @@ def parse_args():
     ap.add_argument("--autotune", action="store_true",
                     help="measure the element kernels' strip shapes on first use (hpc_set_autotune) instead of "
                          "the latency model's choice")
+    ap.add_argument("--tensor-apply", action="store_true",
+                    help="precision form: run the FP32 V-cycle's element operator as TF32 GEMMs on the tensor "
+                         "cores (hpc_set_tensor_apply) instead of the FP32 stencil kernels")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the precision-form measurement on the same increments")
     ap.add_argument("--kernel-only", type=int, default=0, metavar="NB",
@@ -172,13 +175,20 @@ def run_profile_cycles(args, local):
         from hpcrack_b200.solver import precision_mg
         mg_u = precision_mg(w.maxlevel, w.element_nb, K)
     mg_d = tuple(w.mg_d[:4]) + (K,)
+    from hpcrack_b200.solver import KC_MECH_PCG_FINEST, KC_MECH32_PCG_FINEST
+    kc = KC_MECH_PCG_FINEST if args.mech_solver == "fas" else KC_MECH32_PCG_FINEST
+    hier.kernel_timing(kc)  # CUDA-event times of the finest PCG apply (FP64, or FP32 in the precision form)
     launches0 = hier.launch_count()
     outs = [hier.step(t, mg_u, mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du, dU_factor=w.du_factor,
                       mech_tol=w.mech_tol, pf_tol=w.pf_tol, mech_solver=MECH_SOLVERS[args.mech_solver])
             for t in range(2)]
     hier.sync()
+    kn, kms = hier.kernel_time()
     print(json.dumps({"profile_cycles": K, "workload": w.name, "launches": hier.launch_count() - launches0,
-                      "mech_cycles": [int(o[4]) for o in outs], "pf_cycles": [int(o[5]) for o in outs]}), flush=True)
+                      "mech_cycles": [int(o[4]) for o in outs], "pf_cycles": [int(o[5]) for o in outs],
+                      "tensor_apply": TENSOR_APPLY, "finest_pcg_apply": {"launches": kn,
+                                                                         "mean_us": 1000.0 * kms / max(kn, 1)}}),
+          flush=True)
     hier.close()
 
 
@@ -343,10 +353,15 @@ def workload_config(w, world, mech_solver="fas"):
                                      "one FP32 V-cycle (FP64 coarsest solve)"}[mech_solver]}
 
 
+TENSOR_APPLY = False  # --tensor-apply
+
+
 def load_specimen(w, device):
     from hpcrack_b200 import microstructure as ms
     from hpcrack_b200.solver import Hierarchy, H, D
     hier = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start, device=device)
+    if TENSOR_APPLY:
+        hier.set_tensor_apply(True)
     hier.image_material(w.image, w.nodes, w.table(), w.voxel_size)
     if w.crack:
         Hc, dc = ms.precrack_fields(w)
@@ -584,7 +599,9 @@ def run_compare_forms(args, local):
 
 
 def main():
+    global TENSOR_APPLY
     args = parse_args()
+    TENSOR_APPLY = args.tensor_apply
     rank, world, local = dist_setup()
     try:
         if args.kernel_only:

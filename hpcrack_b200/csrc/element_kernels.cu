@@ -140,6 +140,7 @@ struct MechKT {
   const T* rf;
   const T* gpm;  // finest level, precomputed Gauss-point moduli: K at [g * n + e], G at [(8 + g) * n + e]
   RedTarget red;
+  double* err;   // tensor-core kernel: set to 1 when a bounded wait ran out
 };
 using MechK = MechKT<double>;
 
@@ -180,6 +181,82 @@ __device__ __forceinline__ void mech_moduli_finest(const T (&Kn)[8], const T (&G
       Gw[g] = (gd * Gg[g]) * wg;
     }
   }
+}
+
+// Assembly of one row step's element forces f (lane: element x0-1+lane of row ey, layer kk) into
+// nodes: x-neighbours by one shuffle, y-neighbours through the register carry yp, z-neighbours
+// through the warp's shared-memory carry zc; then the epilogue of output node (x, ey, kk) when this
+// row step completes it.
+template <typename T, int EPI, int NF>
+__device__ __forceinline__ void assemble_row(const MechKT<T>& k, const Stream<NF, T>& st, int si, int lane, int x,
+                                             int ey, int kk, int z0, int rr, const T (&f)[3][8], T (&yp)[2][3],
+                                             T* zc, double& red0, double& red1, double& red2) {
+  // ---- combine x-neighbours: node x gets own a=0 corners + left lane's a=1 corners
+  T X[2][2][3];  // [b][c][m]
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const T left = __shfl_up_sync(kFull, f[m][1 + 2 * b + 4 * c], 1);
+        X[b][c][m] = f[m][2 * b + 4 * c] + (lane > 0 ? left : T(0));
+      }
+  if (rr >= 1) {
+    const int orow = rr - 1;
+    T tot[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      T* zp = zc + (orow * 3 + m) * 32 + lane;
+      tot[m] = *zp + yp[0][m] + X[0][0][m];
+      *zp = yp[1][m] + X[0][1][m];
+    }
+    if (kk >= z0 && lane >= 1 && lane <= 30 && x < k.g.nx && ey < k.g.ny) {
+      const long long n = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
+      const long long N = k.g.n;
+      if (EPI == EPI_PLAIN) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m) k.out[n + m * N] = tot[m];
+      } else if (EPI == EPI_RESIDUAL) {
+        const BcFlags bc = bc_flags(k.g, x, ey, kk);
+        const bool fix[3] = {bc.c0, bc.c1, bc.c2};
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          T fv = k.fu[n + m * N];
+          if (k.set_fnorm && fix[m]) {
+            fv = tot[m];
+            k.fu[n + m * N] = fv;
+          }
+          red0 = fma((double)fv, (double)fv, red0);
+          const T rv = fix[m] ? T(0) : fv - tot[m];
+          k.out[n + m * N] = rv;
+          if (k.invM) red1 = fma((double)rv, (double)(rv * k.invM[n + m * N]), red1);
+          red2 = fma((double)rv, (double)rv, red2);
+        }
+      } else if (EPI == EPI_PCG) {  // w = K p, (p, w)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          k.out[n + m * N] = tot[m];
+          red0 = fma((double)st.at(si - 1, m, 0, lane), (double)tot[m], red0);
+        }
+      } else if (EPI == EPI_FAS) {
+        // coarsen_f_standard_routine (multigrid_intergrid.cpp:124-342) fused with the coarse apply
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+          k.out[n + m * N] = tot[m] + full_weight(k.gf, k.rf + (long long)m * k.gf.n, 2 * x, 2 * ey, 2 * kk);
+      } else if (EPI == EPI_REACTION) {
+        // Dirichlet_force_u (boundary_conditions.cpp:69-111)
+        const BcFlags bc = bc_flags(k.g, x, ey, kk);
+        if (bc.c0) k.out[n] = tot[0];
+        if (bc.c1) k.out[n + N] = tot[1];
+        if (bc.c2) k.out[n + 2 * N] = tot[2];
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) yp[c][m] = X[1][c][m];
 }
 
 // T = double: the plain form; T = float: the precision form's V-cycle (reductions stay FP64).
@@ -293,72 +370,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
 #pragma unroll
           for (int n = 0; n < 8; ++n) f[m][n] = T(0);
       }
-      // ---- combine x-neighbours: node x gets own a=0 corners + left lane's a=1 corners
-      T X[2][2][3];  // [b][c][m]
-#pragma unroll
-      for (int c = 0; c < 2; ++c)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-          for (int m = 0; m < 3; ++m) {
-            const T left = __shfl_up_sync(kFull, f[m][1 + 2 * b + 4 * c], 1);
-            X[b][c][m] = f[m][2 * b + 4 * c] + (lane > 0 ? left : T(0));
-          }
-      if (rr >= 1) {
-        const int orow = rr - 1;
-        T tot[3];
-#pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          T* zp = zc + (orow * 3 + m) * 32 + lane;
-          tot[m] = *zp + yp[0][m] + X[0][0][m];
-          *zp = yp[1][m] + X[0][1][m];
-        }
-        if (kk >= z0 && lane >= 1 && lane <= 30 && x < k.g.nx && ey < k.g.ny) {
-          const long long n = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
-          const long long N = k.g.n;
-          if (EPI == EPI_PLAIN) {
-#pragma unroll
-            for (int m = 0; m < 3; ++m) k.out[n + m * N] = tot[m];
-          } else if (EPI == EPI_RESIDUAL) {
-            const BcFlags bc = bc_flags(k.g, x, ey, kk);
-            const bool fix[3] = {bc.c0, bc.c1, bc.c2};
-#pragma unroll
-            for (int m = 0; m < 3; ++m) {
-              T fv = k.fu[n + m * N];
-              if (k.set_fnorm && fix[m]) {
-                fv = tot[m];
-                k.fu[n + m * N] = fv;
-              }
-              red0 = fma((double)fv, (double)fv, red0);
-              const T rv = fix[m] ? T(0) : fv - tot[m];
-              k.out[n + m * N] = rv;
-              if (k.invM) red1 = fma((double)rv, (double)(rv * k.invM[n + m * N]), red1);
-              red2 = fma((double)rv, (double)rv, red2);
-            }
-          } else if (EPI == EPI_PCG) {  // w = K p, (p, w)
-#pragma unroll
-            for (int m = 0; m < 3; ++m) {
-              k.out[n + m * N] = tot[m];
-              red0 = fma((double)st.at(si - 1, m, 0, lane), (double)tot[m], red0);
-            }
-          } else if (EPI == EPI_FAS) {
-            // coarsen_f_standard_routine (multigrid_intergrid.cpp:124-342) fused with the coarse apply
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-              k.out[n + m * N] = tot[m] + full_weight(k.gf, k.rf + (long long)m * k.gf.n, 2 * x, 2 * ey, 2 * kk);
-          } else if (EPI == EPI_REACTION) {
-            // Dirichlet_force_u (boundary_conditions.cpp:69-111)
-            const BcFlags bc = bc_flags(k.g, x, ey, kk);
-            if (bc.c0) k.out[n] = tot[0];
-            if (bc.c1) k.out[n + N] = tot[1];
-            if (bc.c2) k.out[n + 2 * N] = tot[2];
-          }
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 2; ++c)
-#pragma unroll
-        for (int m = 0; m < 3; ++m) yp[c][m] = X[1][c][m];
+      assemble_row<T, EPI, NF>(k, st, si, lane, x, ey, kk, z0, rr, f, yp, zc, red0, red1, red2);
       __syncwarp();
     }
   }
@@ -366,6 +378,335 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
     double v[3] = {red0, red1, red2};
     grid_reduce<3>(v, k.red);
   }
+}
+
+
+// ------------------------------------------------------------------------------------------
+// Tensor-core element contraction (precision form, FP32 with TF32 operands)
+// ------------------------------------------------------------------------------------------
+// The same strips and node assembly as mech_kernel, with the element algebra as two small GEMMs on
+// the 5th-generation tensor cores.  A block's 4 warps march 4 strips in lockstep, so one row step
+// gives 128 elements = 128 rows of an MMA tile (TMEM lane 32w+l = element of lane l of warp w):
+//   strains  D1[e][(g,s)] = sum_k U[e][k] B[(g,s)][k]     128 x 48, K = 24 (3 MMAs of K = 8)
+//   stresses S[e][(g,s)]  = Hooke's law per Gauss point g with that point's moduli (CUDA cores)
+//   forces   D2[e][k]     = sum_(g,s) S[e][(g,s)] B[(g,s)][k]   128 x 24 (N padded to 32), K = 48
+// k = m*8 + n indexes the element's 24 DoFs (component m, node n = a + 2b + 4c), s the 6 engineering
+// strains (xx, yy, zz, xy, xz, yz); B holds the reference-coordinate shape-function derivatives at
+// the 2x2x2 Gauss points (isotropic spacing: the material carries 1/h^2 and the Gauss weight, as in
+// the stencil kernels).  Operands are staged in shared memory in the canonical K-major layout
+// without swizzle (a core matrix = 8 rows x 16 bytes, contiguous); one thread issues the MMAs and
+// commits them to an mbarrier; every thread reads its own element's row back from TMEM.
+// TF32 keeps 10 mantissa bits of each operand: an approximation of the FP32 operator at the 1e-3
+// level, used only inside the preconditioning V-cycle of the flexible-PCG precision form.
+constexpr int kTcCols = 128;                 // TMEM columns per block: D1 at 0..47, D2 at 64..95
+constexpr int kTcD2 = 64;
+constexpr int kTcABytes = 12 * 128 * 16;     // A tile: 128 rows, K up to 48 (12 chunks of 4 values)
+constexpr int kTcB1Bytes = 6 * 48 * 16;      // B for the strains: 48 rows, K = 24
+constexpr int kTcB2Bytes = 12 * 32 * 16;     // B for the forces: 32 rows (24 used), K = 48
+constexpr int kTcHead = kTcABytes + kTcB1Bytes + kTcB2Bytes + 16;  // + mbarrier and TMEM address
+constexpr unsigned kTcWaitPolls = 1u << 24;  // ~0.5 s of polling: far above any MMA's latency
+
+// Shape-function derivative d N_n / d xi_j at Gauss point g, reference coordinates of the element.
+__device__ __forceinline__ float tc_dn(int n, int j, int g, float t0, float t1) {
+  const int a[3] = {n & 1, (n >> 1) & 1, n >> 2};
+  const float tg[3] = {(g & 1) ? t1 : t0, ((g >> 1) & 1) ? t1 : t0, (g >> 2) ? t1 : t0};
+  float v = 1.f;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float shape = a[d] ? tg[d] : 1.f - tg[d];
+    v *= d == j ? (a[d] ? 1.f : -1.f) : shape;
+  }
+  return v;
+}
+// Strain-displacement entry: row (g, s) = g*6 + s, column k = m*8 + n.
+__device__ __forceinline__ float tc_b(int row, int k, float t0, float t1) {
+  const int g = row / 6, sd = row % 6, m = k >> 3, n = k & 7;
+  // derivative direction of component m in strain sd (-1: the component does not enter it):
+  // xx: u_x,x  yy: u_y,y  zz: u_z,z  xy: u_x,y + u_y,x  xz: u_x,z + u_z,x  yz: u_y,z + u_z,y
+  int j = -1;
+  if (sd < 3) j = m == sd ? sd : -1;
+  else if (sd == 3) j = m == 0 ? 1 : (m == 1 ? 0 : -1);
+  else if (sd == 4) j = m == 0 ? 2 : (m == 2 ? 0 : -1);
+  else j = m == 1 ? 2 : (m == 2 ? 1 : -1);
+  return j < 0 ? 0.f : tc_dn(n, j, g, t0, t1);
+}
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);  // version 1, no swizzle
+}
+// kind::tf32, F32 accumulate, both operands K-major, M = 128.
+__host__ __device__ constexpr uint32_t tc_idesc(int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+  for (unsigned i = 0; i < kTcWaitPolls; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16], int o) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  (void)o;
+}
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Row steps a strip of the strip list takes (layers of its z-slab x (wy + 1) staged rows); 0 past the list.
+__device__ __forceinline__ int strip_steps(const StripGeo& sg, const LevelGeo& g, long long strip) {
+  if (strip >= sg.nstrips) return 0;
+  const int sz = (int)(strip / ((long long)sg.tx * sg.ty));
+  const int z0 = sz * sg.cz;
+  const int zend = min(z0 + sg.cz - 1, g.nz - 1);
+  return (zend - z0 + 2) * (sg.wy + 1);
+}
+
+template <bool FINEST, int EPI>
+__global__ void __launch_bounds__(kWarps * 32) mech_tc_kernel(MechKT<float> k) {
+  using T = float;
+  constexpr int NU = 3;
+  constexpr int NF = NU + (FINEST ? 0 : 2);  // the finest level reads precomputed Gauss-point moduli
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  float* As = reinterpret_cast<float*>(tc_smem);
+  float* B1s = reinterpret_cast<float*>(tc_smem + kTcABytes);
+  float* B2s = reinterpret_cast<float*>(tc_smem + kTcABytes + kTcB1Bytes);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tc_smem + kTcABytes + kTcB1Bytes + kTcB2Bytes);
+  uint32_t* taddr_s = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+  T* ring = reinterpret_cast<T*>(tc_smem + kTcHead) + (size_t)wib * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32);
+  T* zc = ring + kRing * NF * 2 * kRowW;
+  const SFt<T> s = make_sf<T>(k.g);
+  const uint32_t sA = (uint32_t)__cvta_generic_to_shared(As), sB1 = (uint32_t)__cvta_generic_to_shared(B1s);
+  const uint32_t sB2 = (uint32_t)__cvta_generic_to_shared(B2s), sbar = (uint32_t)__cvta_generic_to_shared(bar);
+
+  // ---- set-up: the two B operands, the mbarrier, 128 TMEM columns
+  for (int i = tid; i < 48 * 24; i += blockDim.x) {
+    const int r = i / 24, kk = i - r * 24;
+    B1s[(kk >> 2) * 48 * 4 + r * 4 + (kk & 3)] = tc_b(r, kk, s.t[0], s.t[1]);
+  }
+  for (int i = tid; i < 32 * 48; i += blockDim.x) {
+    const int r = i / 48, kk = i - r * 48;
+    B2s[(kk >> 2) * 32 * 4 + r * 4 + (kk & 3)] = r < 24 ? tc_b(kk, r, s.t[0], s.t[1]) : 0.f;
+  }
+  if (wib == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(taddr_s)),
+                 "r"(kTcCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sbar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *taddr_s;
+  const uint32_t trow = tmem + ((uint32_t)(wib * 32) << 16);  // this warp's 32 TMEM lanes
+
+  const T wg = T(k.g.wg) * (s.ih[0] * s.ih[0]);  // isotropic spacing: 1/h^2 in the Gauss weight
+  double red0 = 0.0, red1 = 0.0, red2 = 0.0;
+  const T* fptr[NF];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) fptr[f] = k.fields[f];
+  uint32_t phase = 0;
+  int bad = 0, aborted = 0;
+  const long long nblk_strips = (k.sg.nstrips + kWarps - 1) / kWarps;
+
+  for (long long cs = blockIdx.x; cs < nblk_strips && !aborted; cs += gridDim.x) {
+    const long long strip = cs * kWarps + wib;
+    int steps = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) steps = max(steps, strip_steps(k.sg, k.g, cs * kWarps + w));
+    const bool active = strip < k.sg.nstrips;
+    const long long sref = active ? strip : cs * kWarps;  // inactive warps follow the block's first strip
+    const int sx = (int)(sref % k.sg.tx);
+    const long long rest = sref / k.sg.tx;
+    const int sy = (int)(rest % k.sg.ty);
+    const int sz = (int)(rest / k.sg.ty);
+    const int wy = k.sg.wy, rows = wy + 1;
+    const int x0 = sx * kOX, y0 = sy * (wy - 1), z0 = sz * k.sg.cz;
+    const int x = x0 - 1 + lane;
+    const int zend = min(z0 + k.sg.cz - 1, k.g.nz - 1);
+    Stream<NF, T> st{ring, fptr, x, y0, z0, zend - z0 + 2, 0, rows, &k.g};
+    st.total = active ? st.nlayers * rows : 0;
+    st.issue(0, lane);
+    st.issue(1, lane);
+    T yp[2][3];
+    for (int si = 0; si < steps; ++si) {
+      st.issue(si + 2, lane);
+      cp_async_wait2();
+      __syncwarp();
+      const int li = si / rows, r = si - li * rows;  // the same for the 4 strips: equal shapes
+      const int kk = z0 - 1 + li;
+      if (r == 0) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+          for (int m = 0; m < 3; ++m) yp[c][m] = T(0);
+        __syncwarp();
+        continue;
+      }
+      const bool mine = si < st.total;  // this warp's strip still has this row step
+      const int rr = r - 1, ey = y0 - 1 + rr;
+      const bool valid = mine && lane < 31 && x >= 0 && x <= k.g.nx - 2 && ey >= 0 && ey <= k.g.ny - 2 &&
+                         kk >= 0 && kk <= k.g.nz - 2;
+      const int row = wib * 32 + lane;
+      // this element's moduli, loaded now so that their latency overlaps the strain MMAs
+      T Kw[8], Gw[8];
+      if (valid) {
+        if (FINEST) {
+          const long long el = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
+#pragma unroll
+          for (int g = 0; g < 8; ++g) {
+            Kw[g] = k.gpm[(long long)g * k.g.n + el];
+            Gw[g] = k.gpm[(long long)(8 + g) * k.g.n + el];
+          }
+        } else {
+          const T K = st.at(si - 1, NU + 0, 0, lane) * wg, G = st.at(si - 1, NU + 1, 0, lane) * wg;
+#pragma unroll
+          for (int g = 0; g < 8; ++g) {
+            Kw[g] = K;
+            Gw[g] = G;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int g = 0; g < 8; ++g) Kw[g] = Gw[g] = T(0);
+      }
+      // ---- A = the element's 24 displacement values (zeros for lanes without an element)
+      {
+        T u[24];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+          const int a = n & 1, b = (n >> 1) & 1, c = n >> 2;
+          const int srow = b ? si : si - 1;
+#pragma unroll
+          for (int m = 0; m < 3; ++m) u[m * 8 + n] = valid ? st.at(srow, m, c, lane + a) : T(0);
+        }
+#pragma unroll
+        for (int kc = 0; kc < 6; ++kc)
+          *reinterpret_cast<float4*>(As + kc * 512 + row * 4) =
+              make_float4(u[4 * kc], u[4 * kc + 1], u[4 * kc + 2], u[4 * kc + 3]);
+      }
+      fence_async_smem();
+      tc_fence_before();
+      if (__syncthreads_or(bad)) { aborted = 1; break; }
+      if (tid == 0) {
+        tc_fence_after();
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          tc_mma(tmem, tc_desc(sA + q * 4096, 2048, 128), tc_desc(sB1 + q * 1536, 768, 128), tc_idesc(48), q > 0);
+        tc_commit(sbar);
+      }
+      if (!tc_wait(sbar, phase)) bad = 1;
+      phase ^= 1u;
+      tc_fence_after();
+      // ---- strains of the element at its 8 Gauss points -> stresses
+      float e[48];
+      {
+        float t16[16];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          tc_ld16(trow + q * 16, t16, q);
+          tc_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) e[q * 16 + i] = t16[i];
+        }
+      }
+      {
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+          float* v = e + 6 * g;
+          const T K = Kw[g], G = Gw[g];
+          const T tr = v[0] + v[1] + v[2];
+          const T lt = fmaf(T(-2.0 / 3.0), G, K) * tr;
+          const T G2 = G + G;
+          v[0] = fmaf(G2, v[0], lt);
+          v[1] = fmaf(G2, v[1], lt);
+          v[2] = fmaf(G2, v[2], lt);
+          v[3] *= G;
+          v[4] *= G;
+          v[5] *= G;
+        }
+#pragma unroll
+        for (int kc = 0; kc < 12; ++kc)
+          *reinterpret_cast<float4*>(As + kc * 512 + row * 4) =
+              make_float4(e[4 * kc], e[4 * kc + 1], e[4 * kc + 2], e[4 * kc + 3]);
+      }
+      fence_async_smem();
+      tc_fence_before();
+      if (__syncthreads_or(bad)) { aborted = 1; break; }
+      if (tid == 0) {
+        tc_fence_after();
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+          tc_mma(tmem + kTcD2, tc_desc(sA + q * 4096, 2048, 128), tc_desc(sB2 + q * 1024, 512, 128), tc_idesc(32),
+                 q > 0);
+        tc_commit(sbar);
+      }
+      if (!tc_wait(sbar, phase)) bad = 1;
+      phase ^= 1u;
+      tc_fence_after();
+      T f[3][8];
+      {
+        float a16[16], a8[8];
+        tc_ld16(trow + kTcD2, a16, 0);
+        tc_ld8(trow + kTcD2 + 16, a8);
+        tc_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) f[i >> 3][i & 7] = a16[i];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) f[2][i] = a8[i];
+      }
+      tc_fence_before();
+      if (mine) assemble_row<T, EPI, NF>(k, st, si, lane, x, ey, kk, z0, rr, f, yp, zc, red0, red1, red2);
+      __syncwarp();
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  if (aborted && tid == 0 && k.err) *k.err = 1.0;
+  if (EPI == EPI_RESIDUAL || EPI == EPI_PCG) {
+    double v[3] = {red0, red1, red2};
+    grid_reduce<3>(v, k.red);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (wib == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols));
 }
 
 static int g_num_sms = 0;
@@ -496,12 +837,14 @@ static int autotune_shape(hpc_ctx* c, Kern kern, Args a, size_t smem, long long 
 // of the level comes from the latency model (choose_strips), or from a measurement when the context
 // has autotuning on (first use of a kernel on a level size, outside stream capture) or the process
 // measured it before.
+// `units`: the strip-shape model's parallel units (0: the SM sub-partitions).
 template <class Kern, class Args>
-static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls, int ox = kOX) {
+static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls, int ox = kOX, long long units = 0) {
   int per_sm = 1;
   int rc = kernel_cfg(kern, smem, &per_sm);
   if (rc) return rc;
   const long long cap = (long long)num_sms() * per_sm;
+  if (units <= 0) units = (long long)num_sms() * 4;
   int dev = 0;
   cudaGetDevice(&dev);
   if (!tuned_shape((const void*)kern, dev, a.g, &a.sg, ox)) {
@@ -512,7 +855,7 @@ static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls, in
       if (g_ntuned < 512)
         g_tuned[g_ntuned++] = TunedShape{(const void*)kern, dev, a.g.nx, a.g.ny, a.g.nz, a.sg.wy, a.sg.cz};
     } else {
-      a.sg = choose_strips(a.g, (long long)num_sms() * 4, ox);
+      a.sg = choose_strips(a.g, units, ox);
     }
   }
   const int grid = grid_for(a.sg, cap);
@@ -544,7 +887,8 @@ inline bool iso(const LevelGeo& g) { return g.hx == g.hy && g.hy == g.hz; }
 
 template <bool F, int E, bool D, typename T = double>
 static int run_mech(hpc_ctx* c, const MechKT<T>& k) {
-  const int cls = (F && E == EPI_PCG && !D && sizeof(T) == 8) ? HPC_KC_MECH_PCG_FINEST : HPC_KC_NONE;
+  const int cls = (F && E == EPI_PCG && !D) ? (sizeof(T) == 8 ? HPC_KC_MECH_PCG_FINEST : HPC_KC_MECH32_PCG_FINEST)
+                                             : HPC_KC_NONE;
   if constexpr (F && !D) {
     if (k.gpm) {  // precomputed Gauss-point moduli: only u is staged
       constexpr int NF = 3;
@@ -616,6 +960,15 @@ int launch_mech_diag(hpc_ctx* c, int level, bool finest, double small_k, double*
   return finest ? run_mech<true, EPI_PLAIN, true>(c, k) : run_mech<false, EPI_PLAIN, true>(c, k);
 }
 
+template <bool F, int E>
+static int run_mech_tc(hpc_ctx* c, const MechKT<float>& k) {
+  constexpr int NF = 3 + (F ? 0 : 2);
+  const size_t smem = (size_t)kTcHead + (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(float);
+  // strip shapes of the latency model (one lockstep block per SM on the large levels); shapes that
+  // give every resident block (3 per SM) strips measured slower (MMA round trips share the SM)
+  return launch_strips(c, mech_tc_kernel<F, E>, k, smem, (F && E == EPI_PCG) ? HPC_KC_MECH32_PCG_FINEST : HPC_KC_NONE);
+}
+
 // Single-precision element operator of the precision form's V-cycle: the same kernels on the FP32
 // mirror of a level (LevelF32); residual, PCG apply and FAS right-hand side epilogues.
 int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
@@ -644,7 +997,17 @@ int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
   k.rf = m.rf;
   k.gpm = (m.finest && c->gpm_active) ? F.gpm : nullptr;
   k.red = make_red(c, m.s_out0, m.s_out1, m.s_out2);
+  k.err = c->scal + S_ERR;
   const bool fin = m.finest;
+  // tensor-core contraction (hpc_set_tensor_apply): isotropic levels, Gauss-point moduli at the finest
+  if (c->tc_apply && iso(g) && (!fin || k.gpm)) {
+    switch (m.epi) {
+      case EPI_PLAIN: return fin ? run_mech_tc<true, EPI_PLAIN>(c, k) : run_mech_tc<false, EPI_PLAIN>(c, k);
+      case EPI_RESIDUAL: return fin ? run_mech_tc<true, EPI_RESIDUAL>(c, k) : run_mech_tc<false, EPI_RESIDUAL>(c, k);
+      case EPI_PCG: return fin ? run_mech_tc<true, EPI_PCG>(c, k) : run_mech_tc<false, EPI_PCG>(c, k);
+      case EPI_FAS: return run_mech_tc<false, EPI_FAS>(c, k);
+    }
+  }
   switch (m.epi) {
     case EPI_PLAIN:
       return fin ? run_mech<true, EPI_PLAIN, false>(c, k) : run_mech<false, EPI_PLAIN, false>(c, k);

@@ -784,6 +784,15 @@ static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double
     }
     rel = f_norm != 0 ? rn / f_norm : 1.0;
   }
+  if (mixed && c->tc_apply) {  // the tensor-core applies report a wait that ran out in S_ERR
+    double err = 0.0;
+    if ((rc = read_scalars(c, S_ERR, 1, &err))) return rc;
+    if (err != 0.0) {
+      write_scalar(c, S_ERR, 0.0);
+      set_error("tensor-core element apply: an MMA completion wait ran out");
+      return HPC_ERR_CUDA;
+    }
+  }
   c->f_norm = f_norm;
   // u = x, fu restored; externe_force_nodal (mechanical_right_hnd.cpp:18-38)
   HPC_CUDA(cudaMemcpyAsync(F.u, c->fcg.x, vbytes, cudaMemcpyDeviceToDevice, c->stream));
@@ -1063,6 +1072,12 @@ int hpc_level_dims(hpc_ctx* c, int level, int* n3, double* h3) {
 int hpc_sync(hpc_ctx* c) {
   if (!c) return arg_fail("null context");
   HPC_CUDA(cudaStreamSynchronize(c->stream));
+  return HPC_OK;
+}
+
+int hpc_set_tensor_apply(hpc_ctx* c, int on) {
+  if (!c) return arg_fail("null context");
+  c->tc_apply = on != 0;
   return HPC_OK;
 }
 

@@ -60,6 +60,7 @@ enum Scalar : int {
   S_RES0 = 3,     // generic reduction results
   S_RES1 = 4,
   S_RES2 = 5,
+  S_ERR = 6,      // set to 1 by a kernel whose bounded wait ran out (tensor-core apply)
   S_PCG = 16,     // pcg scratch: rz[-1..kMaxRelax], pw[0..kMaxRelax), rn[0..kMaxRelax)
 };
 constexpr int kMaxRelax = 4096;
@@ -108,6 +109,7 @@ struct hpc_ctx {
   } gmech, gpf, g32;  // g32: FP32 coarse part of the mixed-precision preconditioner
   int use_graphs;
   int autotune;  // measure strip shapes on first use (hpc_set_autotune)
+  int tc_apply;        // precision form: element contraction on the tensor cores (hpc_set_tensor_apply)
   int fused_coarsest;  // coarse-level pcg_u in one block when the level fits (hpc_set_fused_coarsest)
   int gpm_active;      // finest applies read F[maxlevel].gpm (set while a mechanical solve runs)
   // per-class launch timing (hpc_kernel_timing)

@@ -20,7 +20,7 @@ from . import lib as _L
 BULK, G, GC, D, H, FD, KE, GE, R, DOLD, DOLDF = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10
 U, FU, RU, UOLD = 16, 17, 18, 19
 VECTOR_FIELDS = (U, FU, RU, UOLD)
-KC_MECH_PCG_FINEST, KC_PF_PCG_FINEST, KC_MECH_UPDATE_FINEST = 0, 1, 2
+KC_MECH_PCG_FINEST, KC_PF_PCG_FINEST, KC_MECH_UPDATE_FINEST, KC_MECH32_PCG_FINEST = 0, 1, 2, 3
 MECH_FAS, MECH_FCG, MECH_MIXED = 0, 1, 2  # hpc_step_params.mech_solver
 # V-cycle (nu0, nu1, nu2, gamma) of the flexible forms' preconditioner: more post-smoothing than the
 # reference's V(4, 2) pays off once the cycle is a preconditioner (257^3 specimen, precision form:
@@ -146,6 +146,10 @@ class Hierarchy:
         a = np.empty(self.n(level), dtype=np.int16)
         self._c("hpc_download_choice", level, a.ctypes.data_as(C.POINTER(C.c_int16)))
         return a
+
+    def set_tensor_apply(self, on: bool = True):
+        """Precision form: the FP32 V-cycle's element operator on the tensor cores (TF32 GEMMs)."""
+        self._c("hpc_set_tensor_apply", int(bool(on)))
 
     def set_fused_coarsest(self, on: bool):
         """Coarsest-level pcg_u in one thread block (default) or as per-iteration kernels."""

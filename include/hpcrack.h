@@ -128,6 +128,13 @@ int hpc_tuned_shapes(int* out5, int cap, int* count);
  * shared memory (up to about 10^3 nodes); 0 uses the per-iteration kernels.  The two differ only in
  * the order of the same sums. */
 int hpc_set_fused_coarsest(hpc_ctx* ctx, int on);
+/* No counterpart in the reference: 1 runs the element operator of the precision form's FP32 V-cycle
+ * (mech_solver HPC_MECH_MIXED) on the tensor cores - strains and element forces as two TF32 GEMMs
+ * per 128 elements (tcgen05, accumulators in tensor memory), Hooke's law per Gauss point on the
+ * CUDA cores - on levels with equal spacing in x, y and z; 0 (default) keeps the FP32 stencil
+ * kernels.  TF32 operands approximate the FP32 operator to about 1e-3; the flexible PCG around the
+ * V-cycle keeps its FP64 residual, so the solution meets the same tolerance. */
+int hpc_set_tensor_apply(hpc_ctx* ctx, int on);
 /* Kernels launched by this context since the last reset (instrumentation for benchmarks). */
 int hpc_launch_count(hpc_ctx* ctx, long long* count, int reset);
 /* The context's CUDA stream (cudaStream_t), for callers that time on it. */
@@ -137,7 +144,8 @@ enum hpc_kernel_class {
   HPC_KC_NONE = -1,
   HPC_KC_MECH_PCG_FINEST = 0,   /* w = K(d) p and (p, w) on the finest level (FP64) */
   HPC_KC_PF_PCG_FINEST = 1,     /* w = A_d p and (p, w) on the finest level */
-  HPC_KC_MECH_UPDATE_FINEST = 2 /* u += alpha p, r -= alpha w, rz and |r|^2 on the finest level */
+  HPC_KC_MECH_UPDATE_FINEST = 2, /* u += alpha p, r -= alpha w, rz and |r|^2 on the finest level */
+  HPC_KC_MECH32_PCG_FINEST = 3   /* the precision form's FP32 w = K p on the finest level */
 };
 /* Records a start/stop event pair around every launch of `kernel_class` from now on (HPC_KC_NONE
  * stops recording); resets the record. */
