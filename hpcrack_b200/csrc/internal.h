@@ -44,7 +44,7 @@ struct LevelFields {
 };
 
 // Single-precision mirror of one level for the V-cycle of the precision form (hpc_step with
-// mech_solver HPC_MECH_FCG32): vectors 3n floats, material n floats, allocated on first use.
+// mech_solver HPC_MECH_MIXED): vectors 3n floats, material n floats, allocated on first use.
 struct LevelF32 {
   float *u, *fu, *ru, *uold, *p, *w, *invM;  // 3n each; invM: inverse diagonal of K
   float *K, *G, *d;                           // finest level: nodal moduli and phase field
