@@ -14,20 +14,23 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 GEOMS = [
-    (2, (2, 2, 2)),     # 9^3 finest, 3^3 coarsest
-    (2, (4, 3, 5)),     # anisotropic 17 x 13 x 21
-    (1, (8, 2, 3)),     # 17 x 5 x 7 (nx > ny: the MP_choice loop-bound quirk matters)
-    (1, (2, 7, 3)),     # 5 x 15 x 7 (ny > nx)
-    (0, (30, 3, 2)),    # single level, 31 x 4 x 3: strips wider than a warp
+    (2, (2, 2, 2), (0, 0, 0)),     # 9^3 finest, 3^3 coarsest
+    (2, (4, 3, 5), (0, 0, 0)),     # anisotropic 17 x 13 x 21
+    (1, (8, 2, 3), (0, 0, 0)),     # 17 x 5 x 7 (nx > ny: the MP_choice loop-bound quirk matters)
+    (1, (2, 7, 3), (0, 0, 0)),     # 5 x 15 x 7 (ny > nx)
+    (0, (30, 3, 2), (0, 0, 0)),    # single level, 31 x 4 x 3: strips wider than a warp
+    # an image ROI start (input_setting, image_input.cpp:21-27) makes hx, hy, hz differ: the kernels
+    # without the isotropic 1/h^2 folding
+    (1, (4, 3, 2), (1, 2, 0)),     # 9 x 7 x 5, h = (2.25, 2.67, 2) on level 0
 ]
 
 
-@pytest.fixture(params=GEOMS, ids=lambda g: f"L{g[0]}-{g[1][0]}x{g[1][1]}x{g[1][2]}")
+@pytest.fixture(params=GEOMS, ids=lambda g: f"L{g[0]}-{g[1][0]}x{g[1][1]}x{g[1][2]}-roi{g[2][0]}{g[2][1]}{g[2][2]}")
 def pair(request):
-    ml, enb = request.param
+    ml, enb, roi = request.param
     x0 = (-3.0, 1.5, -7.0)
-    gpu = Hierarchy(ml, enb, x0=x0)
-    orc = COracle(ml, enb, x0=x0)
+    gpu = Hierarchy(ml, enb, x0=x0, roi=roi)
+    orc = COracle(ml, enb, x0=x0, roi=roi)
     load_random([gpu, orc], ml, enb, seed=123)
     yield ml, gpu, orc
     gpu.close()

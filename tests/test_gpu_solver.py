@@ -18,9 +18,9 @@ MG_U = (50, 4, 2, 1, 12)
 MG_D = (10, 2, 1, 1, 12)
 
 
-def _pair(ml, enb, seed=7):
-    gpu = Hierarchy(ml, enb)
-    orc = COracle(ml, enb)
+def _pair(ml, enb, seed=7, roi=(0, 0, 0)):
+    gpu = Hierarchy(ml, enb, roi=roi)
+    orc = COracle(ml, enb, roi=roi)
     load_random([gpu, orc], ml, enb, seed)
     return gpu, orc
 
@@ -61,8 +61,11 @@ def test_pcg_d_single():
         assert abs(fg - fo) <= 1e-12 * abs(fo)
 
 
-def test_cycles():
-    gpu, orc = _pair(2, (8, 8, 8))
+@pytest.mark.parametrize("roi", [(0, 0, 0), (3, 1, 2)], ids=["isotropic", "roi-anisotropic"])
+def test_cycles(roi):
+    """V-cycles; an image ROI start makes hx, hy, hz differ on every level (the kernels without the
+    isotropic 1/h^2 folding)."""
+    gpu, orc = _pair(2, (8, 8, 8), roi=roi)
     for impl in (gpu, orc):
         impl.mp_all_element(1e-5)
         impl.vr_all_level(KE)
