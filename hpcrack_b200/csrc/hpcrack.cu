@@ -722,51 +722,68 @@ static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double
   *cycles = 0;
   *fin_iters = 0;
   const int per_cycle = (L == 0) ? mg.nu0 : mg.nu1 + mg.nu2;
+  // The precision form's iteration has no host read until its residual norm: with graphs on (and no
+  // launch timing), each iteration of one class (k = 0, odd k, even k) is captured once and replayed.
+  const bool whole_graph = mixed && c->use_graphs && c->timing_class < 0;
   for (int k = 0; k < mg.ncy; ++k) {
     if (rel <= mech_tol && !(t == 0 && k == 0)) break;  // one iteration forced at t == 0 (:74, :84-85)
-    // z = V-cycle on A z = r from z = 0 with homogeneous Dirichlet values: u is the cycle's unknown,
-    // fu its right-hand side
-    if (mixed) {  // the same cycle on the FP32 mirror; z comes back to F.u in FP64
-      const LevelF32& G = c->F32[L];
-      HPC_CUDA(cudaMemsetAsync(G.u, 0, 3 * (size_t)g.n * sizeof(float), c->stream));
-      if ((rc = launch_to_f32(c, c->fcg.r, G.fu, 3 * g.n))) return rc;
-      if (L == 0) {
-        if ((rc = cycle_u32(c, 0, mg, small_k))) return rc;
+    auto iteration = [&](bool coarse_graph) -> int {
+      int r2;
+      // z = V-cycle on A z = r from z = 0 with homogeneous Dirichlet values: u is the cycle's unknown,
+      // fu its right-hand side
+      if (mixed) {  // the same cycle on the FP32 mirror; z comes back to F.u in FP64
+        const LevelF32& G = c->F32[L];
+        HPC_CUDA(cudaMemsetAsync(G.u, 0, 3 * (size_t)g.n * sizeof(float), c->stream));
+        if ((r2 = launch_to_f32(c, c->fcg.r, G.fu, 3 * g.n))) return r2;
+        if (L == 0) {
+          if ((r2 = cycle_u32(c, 0, mg, small_k))) return r2;
+        } else {
+          if ((r2 = pcg_u32(c, L, small_k, mg.nu1, true))) return r2;
+          if (coarse_graph) {
+            if ((r2 = run_graphed(c, c->g32, mg, small_k, 0.0, k > 0, [&] { return coarse_part_u32(c, L, mg, small_k); })))
+              return r2;
+          } else if ((r2 = coarse_part_u32(c, L, mg, small_k))) {
+            return r2;
+          }
+          if ((r2 = pcg_u32(c, L, small_k, mg.nu2))) return r2;
+        }
+        if ((r2 = launch_to_f64(c, G.u, F.u, 3 * g.n))) return r2;
       } else {
-        if ((rc = pcg_u32(c, L, small_k, mg.nu1, true))) return rc;
-        if ((rc = run_graphed(c, c->g32, mg, small_k, 0.0, k > 0,
-                              [&] { return coarse_part_u32(c, L, mg, small_k); })))
-          return rc;
-        if ((rc = pcg_u32(c, L, small_k, mg.nu2))) return rc;
+        HPC_CUDA(cudaMemsetAsync(F.u, 0, vbytes, c->stream));
+        HPC_CUDA(cudaMemcpyAsync(F.fu, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+        if ((r2 = cycle_u_top(c, mg, small_k, 0.0, 1, k > 0))) return r2;
       }
-      if ((rc = launch_to_f64(c, G.u, F.u, 3 * g.n))) return rc;
-    } else {
-      HPC_CUDA(cudaMemsetAsync(F.u, 0, vbytes, c->stream));
-      HPC_CUDA(cudaMemcpyAsync(F.fu, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
-      if ((rc = cycle_u_top(c, mg, small_k, 0.0, 1, k > 0))) return rc;
+      // delta_k = (z, r_k), gamma_k = (z, r_{k-1}); p = z + beta p
+      if ((r2 = launch_dot2(c, L, F.u, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k))))
+        return r2;
+      if ((r2 = launch_fcg_dir(c, L, F.u, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
+        return r2;
+      // w = K p, (p, w); the smoothers' own p and w are free between V-cycles
+      MechCall q{};
+      q.level = L;
+      q.finest = true;
+      q.epi = EPI_PCG;
+      q.src = c->fcg.p;
+      q.out = F.w;
+      q.small_k = small_k;
+      q.s_out0 = slot_fpw(k);
+      q.s_out1 = q.s_out2 = -1;
+      if ((r2 = launch_mech(c, q))) return r2;
+      // r_{k-1} kept for the flexible beta; x += alpha p, r -= alpha w, alpha = delta_k / (p, w)
+      HPC_CUDA(cudaMemcpyAsync(c->fcg.rp, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+      return launch_mech_update_on(c, L, c->fcg.x, c->fcg.r, c->fcg.p, F.w, F.preMu, slot_fdelta(k), slot_fpw(k),
+                                   slot_fdummy(k), slot_frn(k));
+    };
+    if (whole_graph) {
+      // graph key: the cycle parameters, small_k and the kernel choices baked into the launches
+      const double key = (double)(c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active);
+      hpc_ctx::CoarseGraph& gk = c->gfcg[k == 0 ? 0 : ((k & 1) ? 1 : 2)];
+      if ((rc = run_graphed(c, gk, mg, small_k, key, true, [&] { return iteration(false); }))) return rc;
+    } else if ((rc = iteration(true))) {
+      return rc;
     }
     ++*cycles;
     *fin_iters += per_cycle;
-    // delta_k = (z, r_k), gamma_k = (z, r_{k-1}); p = z + beta p
-    if ((rc = launch_dot2(c, L, F.u, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k)))) return rc;
-    if ((rc = launch_fcg_dir(c, L, F.u, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
-      return rc;
-    // w = K p, (p, w); the smoothers' own p and w are free between V-cycles
-    MechCall q{};
-    q.level = L;
-    q.finest = true;
-    q.epi = EPI_PCG;
-    q.src = c->fcg.p;
-    q.out = F.w;
-    q.small_k = small_k;
-    q.s_out0 = slot_fpw(k);
-    q.s_out1 = q.s_out2 = -1;
-    if ((rc = launch_mech(c, q))) return rc;
-    // r_{k-1} kept for the flexible beta; x += alpha p, r -= alpha w, alpha = delta_k / (p, w)
-    HPC_CUDA(cudaMemcpyAsync(c->fcg.rp, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
-    if ((rc = launch_mech_update_on(c, L, c->fcg.x, c->fcg.r, c->fcg.p, F.w, F.preMu, slot_fdelta(k), slot_fpw(k),
-                                    slot_fdummy(k), slot_frn(k))))
-      return rc;
     // The stopping decision is always taken on the true residual f - K x: at t == 0 it is computed
     // every iteration (f_norm follows the reactions of the current iterate); later the recursive
     // residual is used until it passes the test, then the true one confirms it or replaces it.
@@ -1050,6 +1067,8 @@ int hpc_destroy(hpc_ctx* c) {
       if (p) cudaFree(p);
   }
   if (c->g32.valid) cudaGraphExecDestroy(c->g32.exec);
+  for (auto& gf : c->gfcg)
+    if (gf.valid) cudaGraphExecDestroy(gf.exec);
   if (c->ck.stream) cudaStreamSynchronize(c->ck.stream);
   if (c->ck.dev) cudaFree(c->ck.dev);
   if (c->ck.host) cudaFreeHost(c->ck.host);

@@ -72,11 +72,14 @@ constexpr int kScalarPool = S_FCG + 5 * (kMaxRelax + 2);
 inline int slot_rz(int it) { return S_PCG + 1 + it; }  // it >= -1
 inline int slot_pw(int it) { return S_PCG + (kMaxRelax + 2) + it; }
 inline int slot_rn(int it) { return S_PCG + 2 * (kMaxRelax + 2) + it; }
-inline int slot_fdelta(int k) { return S_FCG + 1 + k; }  // k >= -1
-inline int slot_fgamma(int k) { return S_FCG + (kMaxRelax + 2) + k; }
-inline int slot_fpw(int k) { return S_FCG + 2 * (kMaxRelax + 2) + k; }
-inline int slot_frn(int k) { return S_FCG + 3 * (kMaxRelax + 2) + k; }
-inline int slot_fdummy(int k) { return S_FCG + 4 * (kMaxRelax + 2) + k; }
+// Flexible-PCG scalars of iteration k >= -1: two sets by the parity of k (iteration k reads its own
+// and the previous iteration's), so that every iteration of one parity launches the same arguments
+// and can be replayed from one CUDA graph.
+inline int slot_fdelta(int k) { return S_FCG + (k & 1); }
+inline int slot_fgamma(int k) { return S_FCG + 2 + (k & 1); }
+inline int slot_fpw(int k) { return S_FCG + 4 + (k & 1); }
+inline int slot_frn(int k) { return S_FCG + 6 + (k & 1); }
+inline int slot_fdummy(int k) { return S_FCG + 8 + (k & 1); }
 
 }  // namespace hpc
 
@@ -107,6 +110,7 @@ struct hpc_ctx {
     hpc_mg mg;
     double a, b;  // small_k, Ut (mechanical) or lc (phase field)
   } gmech, gpf, g32;  // g32: FP32 coarse part of the mixed-precision preconditioner
+  CoarseGraph gfcg[3];  // precision form: one whole flexible-PCG iteration (k = 0, odd k, even k >= 2)
   int use_graphs;
   int autotune;  // measure strip shapes on first use (hpc_set_autotune)
   int tc_apply;        // precision form: element contraction on the tensor cores (hpc_set_tensor_apply)
