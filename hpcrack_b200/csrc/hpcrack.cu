@@ -367,11 +367,13 @@ static bool same_mg(const hpc_mg& a, const hpc_mg& b) {
 
 // Runs `body` (a coarse part) through a cached CUDA graph: captured on the first call whose
 // parameters differ from the cached ones (the kernels' first use must already have happened,
-// `allow_capture`), replayed afterwards.  Kernel launches are counted per replay.
+// `allow_capture`), replayed afterwards.  Kernel launches are counted per replay.  A graph is keyed
+// by its parameters and by `flags`, the context's kernel choices baked into its launches.
+static int graph_flags(const hpc_ctx* c) { return c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active; }
 template <class Body>
 static int run_graphed(hpc_ctx* c, hpc_ctx::CoarseGraph& g, const hpc_mg& mg, double a, double b, bool allow_capture,
-                       Body body) {
-  const bool hit = g.valid && same_mg(g.mg, mg) && g.a == a && g.b == b;
+                       Body body, int flags) {
+  const bool hit = g.valid && same_mg(g.mg, mg) && g.a == a && g.b == b && g.flags == flags;
   if (!c->use_graphs || (!hit && !allow_capture)) return body();
   if (!hit) {
     if (g.valid) {
@@ -397,6 +399,7 @@ static int run_graphed(hpc_ctx* c, hpc_ctx::CoarseGraph& g, const hpc_mg& mg, do
     g.mg = mg;
     g.a = a;
     g.b = b;
+    g.flags = flags;
   }
   HPC_CUDA(cudaGraphLaunch(g.exec, c->stream));
   c->launches += g.kernels;
@@ -412,7 +415,7 @@ static int cycle_u_top(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, 
   int rc;
   if ((rc = pcg_u_dev(c, L, small_k, Ut, mg.nu1, t))) return rc;
   if ((rc = run_graphed(c, c->gmech, mg, small_k, Ut, allow_capture,
-                        [&] { return coarse_part_u(c, L, mg, small_k, Ut, t, &it); })))
+                        [&] { return coarse_part_u(c, L, mg, small_k, Ut, t, &it); }, graph_flags(c))))
     return rc;
   return pcg_u_dev(c, L, small_k, Ut, mg.nu2, t);
 }
@@ -423,7 +426,8 @@ static int cycle_d_top(hpc_ctx* c, const hpc_mg& mg, double lc, bool allow_captu
   if (L == 0) return cycle_d_dev(c, 0, mg, lc, &it);
   int rc;
   if ((rc = pcg_d_dev(c, L, lc, mg.nu1))) return rc;
-  if ((rc = run_graphed(c, c->gpf, mg, lc, 0.0, allow_capture, [&] { return coarse_part_d(c, L, mg, lc, &it); })))
+  if ((rc = run_graphed(c, c->gpf, mg, lc, 0.0, allow_capture, [&] { return coarse_part_d(c, L, mg, lc, &it); },
+                        graph_flags(c))))
     return rc;
   for (int i = 1; i <= mg.nu2; ++i)
     if ((rc = pcg_d_dev(c, L, lc, mg.nu2))) return rc;
@@ -740,7 +744,8 @@ static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double
         } else {
           if ((r2 = pcg_u32(c, L, small_k, mg.nu1, true))) return r2;
           if (coarse_graph) {
-            if ((r2 = run_graphed(c, c->g32, mg, small_k, 0.0, k > 0, [&] { return coarse_part_u32(c, L, mg, small_k); })))
+            if ((r2 = run_graphed(c, c->g32, mg, small_k, 0.0, k > 0, [&] { return coarse_part_u32(c, L, mg, small_k); },
+                                  graph_flags(c))))
               return r2;
           } else if ((r2 = coarse_part_u32(c, L, mg, small_k))) {
             return r2;
@@ -776,9 +781,8 @@ static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double
     };
     if (whole_graph) {
       // graph key: the cycle parameters, small_k and the kernel choices baked into the launches
-      const double key = (double)(c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active);
       hpc_ctx::CoarseGraph& gk = c->gfcg[k == 0 ? 0 : ((k & 1) ? 1 : 2)];
-      if ((rc = run_graphed(c, gk, mg, small_k, key, true, [&] { return iteration(false); }))) return rc;
+      if ((rc = run_graphed(c, gk, mg, small_k, 0.0, true, [&] { return iteration(false); }, graph_flags(c)))) return rc;
     } else if ((rc = iteration(true))) {
       return rc;
     }

@@ -109,6 +109,7 @@ struct hpc_ctx {
     int valid;
     hpc_mg mg;
     double a, b;  // small_k, Ut (mechanical) or lc (phase field)
+    int flags;    // kernel choices baked into the launches
   } gmech, gpf, g32;  // g32: FP32 coarse part of the mixed-precision preconditioner
   CoarseGraph gfcg[3];  // precision form: one whole flexible-PCG iteration (k = 0, odd k, even k >= 2)
   int use_graphs;
