@@ -915,6 +915,7 @@ int hpc_footprint(const hpc_geometry* geo, size_t* bytes) {
     total += n * sizeof(float) * (21 + (l == geo->maxlevel ? 3 + 16 : 2));
   }
   total += 6 * (size_t)f.nx * f.ny * f.nz * sizeof(double);
+  total += (size_t)f.nx * f.ny * f.nz * sizeof(double);  // upload staging
   *bytes = total;
   return HPC_OK;
 }
@@ -1055,6 +1056,7 @@ int hpc_destroy(hpc_ctx* c) {
   if (c->counter) cudaFree(c->counter);
   if (c->bc_dev_base) cudaFree(c->bc_dev_base);
   if (c->hscal) cudaFreeHost(c->hscal);
+  if (c->stage) cudaFree(c->stage);
   for (int i = 0; i < 2 * c->tev_cap; ++i) cudaEventDestroy(c->tev[i]);
   delete[] c->tev;
   if (c->gmech.valid) cudaGraphExecDestroy(c->gmech.exec);
@@ -1159,14 +1161,27 @@ int hpc_kernel_time(hpc_ctx* c, long long* launches, double* total_ms) {
   return HPC_OK;
 }
 
+// A dense x-fastest host array into the pitched device array d of a level, asynchronously on the
+// context's stream: one contiguous copy into a dense device buffer and an unpack kernel (a pitched
+// host-to-device copy of short rows runs at a fraction of the link's bandwidth).  The host array
+// must stay valid until the stream has passed the copy.
+static int upload_dense(hpc_ctx* c, int level, double* d, const double* host) {
+  if (!c->stage) {
+    const LevelGeo& f = c->L[c->maxlevel];
+    HPC_CUDA(cudaMalloc((void**)&c->stage, sizeof(double) * (size_t)f.nx * f.ny * f.nz));
+  }
+  const LevelGeo& g = c->L[level];
+  HPC_CUDA(cudaMemcpyAsync(c->stage, host, sizeof(double) * (size_t)g.nx * g.ny * g.nz, cudaMemcpyHostToDevice,
+                           c->stream));
+  return launch_unpack(c, level, c->stage, d);
+}
+
 int hpc_upload(hpc_ctx* c, int field, int level, int comp, const double* host) {
   if (!c || !host) return arg_fail("null argument");
   double* d = component(c, field, level, comp);
   if (!d) return arg_fail("bad field/level/component");
-  const LevelGeo& g = c->L[level];
   HPC_CUDA(cudaSetDevice(c->device));
-  HPC_CUDA(cudaMemcpy2DAsync(d, sizeof(double) * g.px, host, sizeof(double) * g.nx, sizeof(double) * g.nx,
-                             (size_t)g.ny * g.nz, cudaMemcpyHostToDevice, c->stream));
+  if (const int rc = upload_dense(c, level, d, host)) return rc;
   HPC_CUDA(cudaStreamSynchronize(c->stream));
   return HPC_OK;
 }
@@ -1285,11 +1300,9 @@ int hpc_checkpoint_restore(hpc_ctx* c, const double* u, const double* v, const d
                            const double* d, const double* d_old, const double* state6) {
   if (!c || !u || !v || !w || !H || !d || !d_old || !state6) return arg_fail("null argument");
   HPC_CUDA(cudaSetDevice(c->device));
-  const LevelGeo& g = c->L[c->maxlevel];
   const double* src[6] = {u, v, w, H, d, d_old};
   for (int i = 0; i < 6; ++i)
-    HPC_CUDA(cudaMemcpy2DAsync(ck_source(c, i), sizeof(double) * g.px, src[i], sizeof(double) * g.nx,
-                               sizeof(double) * g.nx, (size_t)g.ny * g.nz, cudaMemcpyHostToDevice, c->stream));
+    if (const int rc = upload_dense(c, c->maxlevel, ck_source(c, i), src[i])) return rc;
   HPC_CUDA(cudaStreamSynchronize(c->stream));
   return hpc_set_state(c, state6);
 }

@@ -95,6 +95,7 @@ struct hpc_ctx {
   int device;
   double* scal;          // device scalar pool
   double* hscal;         // pinned host staging for scalar reads
+  double* stage;         // dense finest-size device buffer for uploads (first use)
   double* partials;      // per-block reduction partials
   unsigned int* counter; // last-block-done counter
   size_t partials_cap;   // doubles
@@ -231,6 +232,7 @@ int launch_inject_u_f32(hpc_ctx* c, int lf);             // u_c = u_f(2i), Diric
 int launch_prolong_f32(hpc_ctx* c, int lf);              // u_f += P(u_c - uold_c), Dirichlet rows 0
 int launch_to_f32(hpc_ctx* c, const double* src, float* dst, long long n);
 int launch_to_f64(hpc_ctx* c, const float* src, double* dst, long long n);
+int launch_unpack(hpc_ctx* c, int level, const double* dense, double* dst);
 
 struct PfCall {
   int level;

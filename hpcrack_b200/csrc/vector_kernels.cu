@@ -877,6 +877,25 @@ int launch_to_f32(hpc_ctx* c, const double* src, float* dst, long long n) {
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
 }
+// Dense x-fastest host layout -> the level's pitched layout (the upload's second half: one
+// contiguous host-to-device copy into `dense`, then this kernel on the device).
+__global__ void unpack_kernel(LevelGeo g, const double* dense, double* dst) {
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx);
+    const long long r = q / g.nx;
+    const int j = (int)(r % g.ny), k = (int)(r / g.ny);
+    dst[nidx(g, i, j, k)] = dense[q];
+  }
+}
+
+int launch_unpack(hpc_ctx* c, int level, const double* dense, double* dst) {
+  const LevelGeo& g = c->L[level];
+  unpack_kernel<<<flat_grid((long long)g.nx * g.ny * g.nz), kRowThreads, 0, c->stream>>>(g, dense, dst);
+  HPC_CHECK_LAUNCH(c);
+  return HPC_OK;
+}
+
 int launch_to_f64(hpc_ctx* c, const float* src, double* dst, long long n) {
   convert_kernel<<<flat_grid(n), kRowThreads, 0, c->stream>>>(src, dst, n);
   HPC_CHECK_LAUNCH(c);
