@@ -154,6 +154,9 @@ int hpc_kernel_timing(hpc_ctx* ctx, int kernel_class);
 int hpc_kernel_time(hpc_ctx* ctx, long long* launches, double* total_ms);
 
 /* ---------------- host <-> device (dense x-fastest host arrays) ---------------- */
+/* Both return when the copy is complete.  The first upload allocates a dense finest-size device
+ * buffer (8 bytes per finest node, counted by hpc_footprint): an upload is one contiguous copy into it
+ * and a kernel that spreads it into the padded layout. */
 int hpc_upload(hpc_ctx* ctx, int field, int level, int comp, const double* host);
 int hpc_download(hpc_ctx* ctx, int field, int level, int comp, double* host);
 int hpc_upload_choice(hpc_ctx* ctx, int level, const int16_t* host);
