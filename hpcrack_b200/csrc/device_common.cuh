@@ -289,7 +289,9 @@ __device__ __forceinline__ void gp_material(const T (&v)[8], const SFt<T>& s, T 
 // Element stiffness action K_e u_e for Q1 small-strain elasticity with per-Gauss-point moduli
 // (Internal_Force_element, mechanical_pcg.cpp:114-172): sigma = K tr(eps) I + 2G dev(eps).
 // Kw, Gw already include the Gauss weight wg.
-template <bool ISO = false, typename T>
+// LAM: Kw holds the first Lame coefficient K - 2G/3 (times wg) instead of K, as the precomputed
+// Gauss-point moduli store it (the same fma, done once per solve instead of in every apply).
+template <bool ISO = false, typename T, bool LAM = false>
 __device__ __forceinline__ void mech_element(const T (&u)[3][8], const T (&Kw)[8], const T (&Gw)[8],
                                              const SFt<T>& s, T (&f)[3][8]) {
   T gx[3][4], gy[3][4], gz[3][4];
@@ -313,7 +315,7 @@ __device__ __forceinline__ void mech_element(const T (&u)[3][8], const T (&Kw)[8
         const T gyz = gy[2][iy] + gz[1][iz];
         const T K = Kw[g], G = Gw[g];
         const T tr = exx + eyy + ezz;
-        const T lt = fma(T(-2.0 / 3.0), G, K) * tr;
+        const T lt = (LAM ? K : fma(T(-2.0 / 3.0), G, K)) * tr;
         const T G2 = G + G;
         const T sxx = fma(G2, exx, lt), syy = fma(G2, eyy, lt), szz = fma(G2, ezz, lt);
         const T sxy = G * gxy, sxz = G * gxz, syz = G * gyz;

@@ -138,7 +138,7 @@ struct MechKT {
   int set_fnorm;
   const T* invM;
   const T* rf;
-  const T* gpm;  // finest level, precomputed Gauss-point moduli: K at [g * n + e], G at [(8 + g) * n + e]
+  const T* gpm;  // finest level, precomputed Gauss-point moduli: K - 2G/3 at [g * n + e], G at [(8 + g) * n + e]
   RedTarget red;
   double* err;   // tensor-core kernel: set to 1 when a bounded wait ran out
 };
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
 #pragma unroll
             for (int m = 0; m < 3; ++m) u[m][n] = st.at(srow, m, c, lane + a);
           }
-          mech_element<ISO>(u, Kw, Gw, s, f);
+          mech_element<ISO, T, FINEST && GPM>(u, Kw, Gw, s, f);
         }
       } else {
 #pragma unroll
@@ -653,7 +653,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_tc_kernel(MechKT<float> k) {
           float* v = e + 6 * g;
           const T K = Kw[g], G = Gw[g];
           const T tr = v[0] + v[1] + v[2];
-          const T lt = fmaf(T(-2.0 / 3.0), G, K) * tr;
+          const T lt = (FINEST ? K : fmaf(T(-2.0 / 3.0), G, K)) * tr;  // the finest moduli hold K - 2G/3
           const T G2 = G + G;
           v[0] = fmaf(G2, v[0], lt);
           v[1] = fmaf(G2, v[1], lt);
@@ -1043,7 +1043,7 @@ __global__ void gp_material_kernel(LevelGeo g, const T* K, const T* G, const T* 
     mech_moduli_finest(Kn, Gn, dn, choice[e], T(small_k), wg, s, Kw, Gw);
 #pragma unroll
     for (int q8 = 0; q8 < 8; ++q8) {
-      gpm[(long long)q8 * g.n + e] = Kw[q8];
+      gpm[(long long)q8 * g.n + e] = fma(T(-2.0 / 3.0), Gw[q8], Kw[q8]);  // K - 2G/3
       gpm[(long long)(8 + q8) * g.n + e] = Gw[q8];
     }
   }
