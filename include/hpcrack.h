@@ -106,7 +106,11 @@ enum { HPC_MECH_FAS = 0, HPC_MECH_FCG = 1, HPC_MECH_MIXED = 2 };
 /* Allocates the device mirrors of the whole hierarchy on `device`. */
 int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device);
 int hpc_destroy(hpc_ctx* ctx);
-/* Device bytes hpc_create would allocate for this geometry (admission by HBM footprint). */
+/* Device bytes a context of this geometry holds at most while it solves (admission by HBM
+ * footprint): what hpc_create allocates plus everything allocated on first use by the solves, the
+ * precision form, checkpoints and uploads.  Not included: the VTK character buffers of
+ * hpc_vtk_write (up to 16 bytes per node of the written level) and the tensor-core kernel's
+ * per-block tensor memory. */
 int hpc_footprint(const hpc_geometry* geo, size_t* bytes);
 /* Level geometry as initialize() builds it (initialization.cpp:19-134). */
 int hpc_level_dims(hpc_ctx* ctx, int level, int* n3, double* h3);
