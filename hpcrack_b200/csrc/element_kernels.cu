@@ -227,11 +227,11 @@ __device__ __forceinline__ void assemble_row(const MechKT<T>& k, const Stream<NF
             fv = tot[m];
             k.fu[n + m * N] = fv;
           }
-          red0 = fma((double)fv, (double)fv, red0);
+          if (k.red.slot[0] >= 0) red0 = fma((double)fv, (double)fv, red0);  // sums nobody reads are skipped
           const T rv = fix[m] ? T(0) : fv - tot[m];
           k.out[n + m * N] = rv;
           if (k.invM) red1 = fma((double)rv, (double)(rv * k.invM[n + m * N]), red1);
-          red2 = fma((double)rv, (double)rv, red2);
+          if (k.red.slot[2] >= 0) red2 = fma((double)rv, (double)rv, red2);
         }
       } else if (EPI == EPI_PCG) {  // w = K p, (p, w)
 #pragma unroll

@@ -752,17 +752,25 @@ static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double
           }
           if ((r2 = pcg_u32(c, L, small_k, mg.nu2))) return r2;
         }
-        if ((r2 = launch_to_f64(c, G.u, F.u, 3 * g.n))) return r2;
       } else {
         HPC_CUDA(cudaMemsetAsync(F.u, 0, vbytes, c->stream));
         HPC_CUDA(cudaMemcpyAsync(F.fu, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
         if ((r2 = cycle_u_top(c, mg, small_k, 0.0, 1, k > 0))) return r2;
       }
-      // delta_k = (z, r_k), gamma_k = (z, r_{k-1}); p = z + beta p
-      if ((r2 = launch_dot2(c, L, F.u, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k))))
-        return r2;
-      if ((r2 = launch_fcg_dir(c, L, F.u, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
-        return r2;
+      // delta_k = (z, r_k), gamma_k = (z, r_{k-1}); p = z + beta p.  The precision form reads z from the
+      // FP32 cycle directly (its FP64 copy would be exact).
+      if (mixed) {
+        const float* z = c->F32[L].u;
+        if ((r2 = launch_dot2(c, L, z, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k))))
+          return r2;
+        if ((r2 = launch_fcg_dir(c, L, z, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
+          return r2;
+      } else {
+        if ((r2 = launch_dot2(c, L, F.u, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k))))
+          return r2;
+        if ((r2 = launch_fcg_dir(c, L, F.u, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
+          return r2;
+      }
       // w = K p, (p, w); the smoothers' own p and w are free between V-cycles
       MechCall q{};
       q.level = L;

@@ -258,9 +258,12 @@ int launch_mech_update_on(hpc_ctx* c, int level, double* x, double* r, const dou
                           const double* invM, int s_num, int s_den, int s_rz_next, int s_rn);
 // sums (a, b) and (a, c) over a 3n vector of a level into scal[s0], scal[s1] (c may be null)
 int launch_dot2(hpc_ctx* c, int level, const double* a, const double* b, const double* cv, int s0, int s1);
+int launch_dot2(hpc_ctx* c, int level, const float* a, const double* b, const double* cv, int s0, int s1);
 // flexible direction p = z + beta p, beta = (scal[s_delta] - scal[s_gamma]) / scal[s_delta_prev]
 // (Polak-Ribiere form of flexible CG), beta = 0 if first
 int launch_fcg_dir(hpc_ctx* c, int level, const double* z, double* p, bool first, int s_delta, int s_gamma,
+                   int s_delta_prev);
+int launch_fcg_dir(hpc_ctx* c, int level, const float* z, double* p, bool first, int s_delta, int s_gamma,
                    int s_delta_prev);
 int launch_pf_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
 // p = r M^-1 + beta p (beta = scal[s_rz]/scal[s_rz_prev], 0 if first), in place

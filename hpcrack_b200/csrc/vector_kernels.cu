@@ -126,14 +126,17 @@ int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_p
 // ---------------------------------------------------------------------------------------------
 // Flexible PCG of the precision form: two dot products in one pass, the flexible direction update
 // ---------------------------------------------------------------------------------------------
-__global__ void dot2_kernel(LevelGeo g, const double* a, const double* b, const double* cv, RedTarget red) {
+// TA = float: the precision form's z straight from the FP32 V-cycle (its FP64 copy is exact, so the
+// sums are the same bits without the conversion pass).
+template <typename TA>
+__global__ void dot2_kernel(LevelGeo g, const TA* a, const double* b, const double* cv, RedTarget red) {
   double s0 = 0.0, s1 = 0.0;
   FOR_NODES(g) {
     const long long n = nidx(g, i, j, kz);
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
       const long long o = n + (long long)m * g.n;
-      const double av = a[o];
+      const double av = (double)a[o];
       s0 = fma(av, b[o], s0);
       if (cv) s1 = fma(av, cv[o], s1);
     }
@@ -142,14 +145,22 @@ __global__ void dot2_kernel(LevelGeo g, const double* a, const double* b, const 
   grid_reduce<2>(v, red);
 }
 
-int launch_dot2(hpc_ctx* c, int level, const double* a, const double* b, const double* cv, int s0, int s1) {
+template <typename TA>
+static int launch_dot2_t(hpc_ctx* c, int level, const TA* a, const double* b, const double* cv, int s0, int s1) {
   const LevelGeo& g = c->L[level];
-  dot2_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, a, b, cv, make_red(c, s0, cv ? s1 : -1, -1));
+  dot2_kernel<TA><<<row_grid(g), kRowThreads, 0, c->stream>>>(g, a, b, cv, make_red(c, s0, cv ? s1 : -1, -1));
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
 }
+int launch_dot2(hpc_ctx* c, int level, const double* a, const double* b, const double* cv, int s0, int s1) {
+  return launch_dot2_t(c, level, a, b, cv, s0, s1);
+}
+int launch_dot2(hpc_ctx* c, int level, const float* a, const double* b, const double* cv, int s0, int s1) {
+  return launch_dot2_t(c, level, a, b, cv, s0, s1);
+}
 
-__global__ void fcg_dir_kernel(LevelGeo g, const double* z, double* p, int first, const double* scal, int s_delta,
+template <typename TZ>
+__global__ void fcg_dir_kernel(LevelGeo g, const TZ* z, double* p, int first, const double* scal, int s_delta,
                                int s_gamma, int s_delta_prev) {
   const double beta = first ? 0.0 : (scal[s_delta] - scal[s_gamma]) / scal[s_delta_prev];
   FOR_NODES(g) {
@@ -157,18 +168,28 @@ __global__ void fcg_dir_kernel(LevelGeo g, const double* z, double* p, int first
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
       const long long o = n + (long long)m * g.n;
-      p[o] = first ? z[o] : fma(beta, p[o], z[o]);
+      const double zv = (double)z[o];
+      p[o] = first ? zv : fma(beta, p[o], zv);
     }
   }
 }
 
-int launch_fcg_dir(hpc_ctx* c, int level, const double* z, double* p, bool first, int s_delta, int s_gamma,
-                   int s_delta_prev) {
+template <typename TZ>
+static int launch_fcg_dir_t(hpc_ctx* c, int level, const TZ* z, double* p, bool first, int s_delta, int s_gamma,
+                            int s_delta_prev) {
   const LevelGeo& g = c->L[level];
-  fcg_dir_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, z, p, first ? 1 : 0, c->scal, s_delta, s_gamma,
-                                                            s_delta_prev);
+  fcg_dir_kernel<TZ><<<row_grid(g), kRowThreads, 0, c->stream>>>(g, z, p, first ? 1 : 0, c->scal, s_delta, s_gamma,
+                                                                s_delta_prev);
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
+}
+int launch_fcg_dir(hpc_ctx* c, int level, const double* z, double* p, bool first, int s_delta, int s_gamma,
+                   int s_delta_prev) {
+  return launch_fcg_dir_t(c, level, z, p, first, s_delta, s_gamma, s_delta_prev);
+}
+int launch_fcg_dir(hpc_ctx* c, int level, const float* z, double* p, bool first, int s_delta, int s_gamma,
+                   int s_delta_prev) {
+  return launch_fcg_dir_t(c, level, z, p, first, s_delta, s_gamma, s_delta_prev);
 }
 
 __global__ void pf_update_kernel(LevelGeo g, double* d, double* r, const double* p, const double* w,
