@@ -33,16 +33,24 @@ if ROOT not in sys.path:
 METRIC = "MDoF-iter/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
-# Algorithmic bytes per finest node of the PCG apply during a mechanical solve: p and w (24 B each)
-# and the precomputed Gauss-point moduli K_g, G_g (16 doubles per element = 128 B).  (The nodal
-# form that interpolates K, G, d and the regime in the apply itself reads 73 B/node.)
+# Algorithmic bytes per finest node of the mechanical operator apply: u in (24), bulK, G, d (24),
+# the regime (2) and the result (24) = 74 B/node, the compulsory traffic of y = K(d) u.  The roofline
+# is reported on this basis.  The apply as the mechanical solves run it reads the Gauss-point moduli
+# precomputed once per solve instead of bulK, G, d and the regime: p and w (24 B each) plus K_g, G_g
+# (16 doubles per element = 128 B) = 176 B/node, reported beside it (the kernel trades FP64
+# instructions, its bound, for bytes).
+APPLY_BYTES_PER_NODE = 74
 PCG_APPLY_BYTES_PER_NODE = 176
+# ncu counters of the FP64 apply (one capture of the 193^3 level, the same kernel the bench times):
+# FP64 pipe active 60.7 % of active cycles, issue active 56.1 %, top stall "wait" (fixed-latency
+# dependencies) 1.36 per issued instruction.
+APPLY_FP64_PIPE_ACTIVE = 0.607
 MECH_SOLVERS = {"fas": 0, "fcg": 1, "mixed": 2}
 
-# DRAM bytes (read + write) per launch of the finest PCG apply: the ncu capture of
-# profiles/mech_pcg_apply_mid193.md measured 1339.8 MB + 165.9 MB on the 193^3 level (7,189,057
-# nodes, 209.4 B/node: the Gauss-point moduli of strip-edge elements are read twice); other sizes
-# scale that per-node figure by their node count.
+# DRAM bytes (read + write) per launch of the finest PCG apply: one ncu capture of the kernel on the
+# 193^3 level (7,189,057 nodes) measured 1339.8 MB read + 165.9 MB written, 209.4 B/node (the
+# Gauss-point moduli of strip-edge elements are read twice); other sizes scale that per-node figure
+# by their node count.
 PCG_APPLY_TRAFFIC_PER_NODE = (1339.779e6 + 165.902848e6) / 193 ** 3
 
 
@@ -428,7 +436,8 @@ def run_b200(args, rank, world, local):
     clocks = sampler.stop()
     launches = hier.launch_count() - launches0
     ms_total = e0.elapsed_time(e1)
-    u_plain_final = hier.get(U, w.maxlevel) if (not args.no_forms and args.mech_solver == "fas") else None
+    plain_final = ({k: hier.get(f, w.maxlevel) for k, f in (("u", U), ("d", D), ("H", H))}
+                   if (not args.no_forms and args.mech_solver == "fas") else None)
     kn, kms = hier.kernel_time() if not args.no_kernel_timing else (0, 0.0)
     hier.kernel_timing(-1)
 
@@ -441,14 +450,22 @@ def run_b200(args, rank, world, local):
     # (PCG_APPLY_BYTES_PER_NODE algorithmic bytes per finest node).
     roofline = None
     if kn > 0:
-        bytes_total = N * PCG_APPLY_BYTES_PER_NODE * kn
-        achieved = bytes_total / (kms / 1e3) / 1e9
+        achieved = N * APPLY_BYTES_PER_NODE / (kms / kn / 1e3) / 1e9
+        achieved_read = N * PCG_APPLY_BYTES_PER_NODE / (kms / kn / 1e3) / 1e9
         peak, src = peaks()
         roofline = {"bound": "hbm", "kernel": "mech_kernel<finest, PCG, Gauss-point moduli> (w = K(d) p, (p, w))",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "peak_source": src, "traffic": PCG_APPLY_TRAFFIC_PER_NODE * N,
-                    "traffic_note": "bytes per launch: ncu dram bytes per node of the 193^3 capture x nodes",
-                    "launches": kn, "avg_launch_ms": kms / kn, "bytes_per_node": PCG_APPLY_BYTES_PER_NODE}
+                    "peak_source": src, "bytes_per_node": APPLY_BYTES_PER_NODE,
+                    "bytes_basis": "algorithmic: u 24 + bulK,G,d 24 + regime 2 + out 24 B per finest node",
+                    "traffic": PCG_APPLY_TRAFFIC_PER_NODE * N,
+                    "traffic_note": "bytes per launch: ncu dram bytes per node of the 193^3 capture x nodes; above "
+                                    "the 74 B/node because the kernel reads precomputed Gauss-point moduli",
+                    "read_layout": {"bytes_per_node": PCG_APPLY_BYTES_PER_NODE, "achieved": achieved_read,
+                                    "frac": achieved_read / peak,
+                                    "what": "p, w and the precomputed Gauss-point moduli the kernel reads"},
+                    "fp64_pipe_active_ncu": APPLY_FP64_PIPE_ACTIVE,
+                    "limiter": "FP64 pipe (dependent FP64 latency), not HBM",
+                    "launches": kn, "avg_launch_ms": kms / kn}
 
     # ------------------------------------------------------------ end to end through the C ABI
     e2e = None
@@ -525,7 +542,7 @@ def run_b200(args, rank, world, local):
         torch.cuda.synchronize()
         barrier(world)
         p_ms, _ = replicas.aggregate(g0.elapsed_time(g1), 0.0, world)
-        u_mixed = hp.get(U, wp.maxlevel)
+        mixed_final = {k: hp.get(f, wp.maxlevel) for k, f in (("u", U), ("d", D), ("H", H))}
         hp.close()
         forms = {"plain": {"solves_per_s": world * args.steps / (max_ms / 1e3),
                            "v_cycles": [int(o[4]) for o in outs]},
@@ -535,10 +552,11 @@ def run_b200(args, rank, world, local):
                                    "FP32 V-cycle per iteration (FP64 coarsest solve); same increments, same "
                                    "FP64 stopping test |r|/|f| <= 1e-8"},
                  "speedup_mixed_vs_plain": max_ms / p_ms}
-        if u_plain_final is not None:
-            import numpy as np
-            forms["mixed"]["u_rel_l2_vs_plain"] = float(np.linalg.norm(u_mixed - u_plain_final) /
-                                                        np.linalg.norm(u_plain_final))
+        if plain_final is not None:
+            forms["mixed"]["u_rel_l2_vs_plain"] = field_errors(mixed_final["u"], plain_final["u"])["rel_l2"]
+            forms["mixed"]["error_vs_plain"] = {k: field_errors(mixed_final[k], plain_final[k]) for k in ("u", "d", "H")}
+            forms["mixed"]["error_note"] = (f"fields after increment {t_first + args.steps - 1} of both forms, each "
+                                            "solved to |r|/|f| <= 1e-8; rel_l2 = |a-b|/|b|, max_abs = max|a-b|")
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
@@ -553,6 +571,14 @@ def run_b200(args, rank, world, local):
                                   "mech_iters": int(o[6]), "pf_iters": int(o[7]), "F": o[1], "dmax": o[3]}
                                  for i, o in enumerate(outs)]}
         print(json.dumps(line), flush=True)
+
+
+def field_errors(a, b) -> dict:
+    """Relative L2 and maximum absolute difference of field a against field b."""
+    import numpy as np
+    nb = float(np.linalg.norm(b))
+    return {"rel_l2": float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0),
+            "max_abs": float(np.max(np.abs(a - b))), "max_ref": float(np.max(np.abs(b)))}
 
 
 def run_compare_forms(args, local):
@@ -582,12 +608,7 @@ def run_compare_forms(args, local):
                                                               (("u", U), ("d", D), ("H", H))}}
         hier.close()
     plain, other = res["fas"], res[[k for k in res if k != "fas"][0]]
-    errs = {}
-    for k in ("u", "d", "H"):
-        a, b = other["fields"][k], plain["fields"][k]
-        nb = float(np.linalg.norm(b))
-        errs[k] = {"rel_l2": float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0),
-                   "max_abs": float(np.max(np.abs(a - b))), "max_ref": float(np.max(np.abs(b)))}
+    errs = {k: field_errors(other["fields"][k], plain["fields"][k]) for k in ("u", "d", "H")}
     line = {"metric": "solves/s", "workload": w.name, "increments": args.steps,
             "plain": {"solves_per_s": args.steps / (plain["ms"] / 1e3), "ms": plain["ms"],
                       "v_cycles": [int(o[4]) for o in plain["outs"]]},

@@ -1147,6 +1147,18 @@ int hpc_launch_count(hpc_ctx* c, long long* count, int reset) {
 
 void* hpc_stream(hpc_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
+int hpc_binary_version(int* version) {
+  if (!version) return arg_fail("null pointer");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device: the library has no CPU path");
+    return HPC_ERR_NODEVICE;
+  }
+  HPC_CUDA(kernel_binary_version(version));
+  return HPC_OK;
+}
+
 int hpc_kernel_timing(hpc_ctx* c, int kernel_class) {
   if (!c) return arg_fail("null context");
   HPC_CUDA(cudaStreamSynchronize(c->stream));

@@ -278,6 +278,7 @@ int launch_dot(hpc_ctx* c, int level, int ncomp, const double* a, const double* 
 int launch_fill(hpc_ctx* c, double* v, long long n, double value);
 // v = 1/v on the valid nodes of a level (ncomp components)
 int launch_invert(hpc_ctx* c, int level, int ncomp, double* v);
+cudaError_t kernel_binary_version(int* version);
 int launch_axpby(hpc_ctx* c, double* y, const double* a, const double* b, double sa, double sb, long long n);
 // Transfers
 int launch_inject(hpc_ctx* c, int lf, const double* f, double* co, int ncomp);

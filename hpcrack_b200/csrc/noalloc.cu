@@ -13,10 +13,17 @@
 //   * n is limited to kDmaxMaxBlocks * kDmaxPerBlock = 134,217,728 values (a 512^3-node level);
 //     larger n is rejected with HPC_ERR_ARG;
 //   * the first call on a device looks up the scratch address with cudaGetSymbolAddress, with that
-//     device current, and checks the result; later calls on that device reuse the address;
+//     device current, and checks the result; later calls on that device reuse the address.  With
+//     lazy module loading (the CUDA 12 default) that first lookup can be what loads this library's
+//     device code and places the scratch, so the first call may allocate and synchronise: make one
+//     warm-up call (or any other call of this library on that device) before a region that must
+//     not allocate, and before any stream capture.  The cached address does not survive
+//     cudaDeviceReset (the caller must not reset a device it keeps using this library on);
 //   * every call shares the scratch: calls that overlap on the GPU race.  The counter is cleared
 //     by each call before its kernel, so a call never depends on what the previous call left.
 #include <cuda_runtime.h>
+
+#include <atomic>
 
 #include "device_common.cuh"
 #include "internal.h"
@@ -34,7 +41,9 @@ constexpr long long kScratchDoubles = 2 * kDmaxMaxBlocks + 32;                 /
 static __device__ __align__(256) double g_dmax_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
-double* g_scratch_ptr[kMaxDevices] = {nullptr};
+// Per-device scratch address.  Two threads making their first call on one device at once both look
+// the address up and store the same value; the atomic makes that race well defined.
+std::atomic<double*> g_scratch_ptr[kMaxDevices] = {};
 
 // out[0] = max(0, max(d - d_old)), out[1] = max(0, max(d)) (phase_field_max_search.cpp:17-53).
 __global__ void __launch_bounds__(kDmaxThreads) dmax_noalloc_kernel(const double* d, const double* d_old, long long n,
@@ -113,13 +122,14 @@ extern "C" int hpc_dmax_noalloc(const double* d, const double* d_old, long long 
     set_error("hpc_dmax_noalloc: device index beyond the supported range");
     return HPC_ERR_ARG;
   }
-  if (!g_scratch_ptr[dev]) {  // one-time set-up on this device (the current one)
+  double* scratch = g_scratch_ptr[dev].load(std::memory_order_acquire);
+  if (!scratch) {  // one-time set-up on this device (the current one)
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_dmax_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "hpc_dmax_noalloc: cudaGetSymbolAddress");
-    g_scratch_ptr[dev] = static_cast<double*>(p);
+    scratch = static_cast<double*>(p);
+    g_scratch_ptr[dev].store(scratch, std::memory_order_release);
   }
-  double* scratch = g_scratch_ptr[dev];
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   e = cudaMemsetAsync(scratch + 2 * kDmaxMaxBlocks, 0, sizeof(unsigned int), s);
   if (e != cudaSuccess) return cuda_fail(e, "hpc_dmax_noalloc: clearing the counter");

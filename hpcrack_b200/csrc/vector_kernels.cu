@@ -322,6 +322,15 @@ int launch_invert(hpc_ctx* c, int level, int ncomp, double* v) {
   return HPC_OK;
 }
 
+// The compute capability the library's device code was built for, as the runtime reports it for
+// one of its kernels (major * 10 + minor; 100 for sm_100a).
+cudaError_t kernel_binary_version(int* version) {
+  cudaFuncAttributes a{};
+  const cudaError_t e = cudaFuncGetAttributes(&a, invert_kernel);
+  if (e == cudaSuccess) *version = a.binaryVersion;
+  return e;
+}
+
 __global__ void axpby_kernel(double* y, const double* a, const double* b, double sa, double sb, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     y[i] = sa * a[i] + (b ? sb * b[i] : 0.0);

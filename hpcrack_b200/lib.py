@@ -63,6 +63,7 @@ SIGNATURES = {
     "hpc_set_tensor_apply": [_ctx, _i],
     "hpc_tuned_shapes": [_ip, _i, _ip],
     "hpc_launch_count": [_ctx, C.POINTER(C.c_longlong), _i],
+    "hpc_binary_version": [_ip],
     "hpc_stream": [_ctx],
     "hpc_kernel_timing": [_ctx, _i],
     "hpc_kernel_time": [_ctx, C.POINTER(C.c_longlong), _dp],

@@ -193,6 +193,8 @@ def make_workload(name: str) -> Workload:
       pre-crack at mid-height over half the x width; 20 increments.
     * ``mid129`` / ``mid193``  the plain257 recipe scaled to 129^3 / 193^3 (193: element_nb 12), for
       profiling at a few GB of device memory.
+    * ``crack33`` / ``crack65``  the plain257 recipe (three phases, pre-crack) scaled to 33^3 / 65^3,
+      the parity cases of the benchmarked configuration (the reference finishes them in minutes).
     * ``large513``  513^3, seed 2, inclusions to 30 %.
     * ``small17`` / ``small33`` test-sized variants of parity65.
     """
@@ -203,12 +205,14 @@ def make_workload(name: str) -> Workload:
         return Workload(name, img, (8, 8, 8), maxlevel_for(n, 0, 8), (0.0, 0.0, 0.0), 1e-6, 2.0, 1e-6,
                         (50, 4, 2, 1, 200), (10, 2, 1, 1, 200), 3, ut0=1e-4 * (n - 1), du=1e-4 * (n - 1),
                         mech_tol=1e-16, pf_tol=1e-16)
-    if name in ("plain257", "mid129", "mid193"):
-        n = {"plain257": 257, "mid129": 129, "mid193": 193}[name]
+    if name in ("plain257", "mid129", "mid193", "crack33", "crack65"):
+        n = {"plain257": 257, "mid129": 129, "mid193": 193, "crack33": 33, "crack65": 65}[name]
         enb = 12 if n == 193 else 8  # 193 = 12 * 2^4 + 1
         s = (n - 1) / 256.0
-        img = sphere_image((n, n, n), 1, [Phase(INCLUSION_GRAY, 6 * s, 20 * s, volume_fraction=0.25),
-                                          Phase(PORE_GRAY, max(3 * s, 1.5), 8 * s, volume_fraction=0.05)])
+        # radii floors only bind below 129^3 (crack33 / crack65 keep spheres a few voxels wide)
+        img = sphere_image((n, n, n), 1, [Phase(INCLUSION_GRAY, max(6 * s, 2.0), max(20 * s, 4.0),
+                                                volume_fraction=0.25),
+                                          Phase(PORE_GRAY, max(3 * s, 1.5), max(8 * s, 2.5), volume_fraction=0.05)])
         return Workload(name, img, (enb, enb, enb), maxlevel_for(n, 0, enb), (0.0, 0.0, 0.0), 1e-6, 2.0, 1e-6,
                         (50, 4, 2, 1, 200), (10, 2, 1, 1, 200), 20, ut0=1e-4 * (n - 1), du=1e-4 * (n - 1),
                         mech_tol=1e-16, pf_tol=1e-16, crack={"H": 1e6, "layer": (n - 1) // 2, "xfrac": 0.5})

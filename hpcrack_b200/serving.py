@@ -15,6 +15,12 @@ through a number of staggered increments (the loop of crack_propagation.cpp:65-1
 
 Each context's kernels are deterministic and contexts share no device state, so a request's result
 is the same bit for bit whether it runs alone or in a mix; ``tests/test_gpu_serving.py`` checks this.
+That holds with the strip shapes fixed in advance, as they are by default (the latency model).  With
+autotuning on (``hpc_set_autotune``) the first context to meet a level size measures the shapes under
+whatever load is running then and every later context reuses them; a different shape changes the
+summation order, so a request's bits can then differ between a run alone and a run in a mix (both
+still meet the same stopping test).  A server that wants autotuned shapes and bit-reproducible
+requests tunes every size once before admitting requests.
 
 The solver is pluggable (``solver_factory``): the CUDA library's :class:`~hpcrack_b200.solver.Hierarchy`
 in production, any object with the same ``image_material`` / ``set`` / ``voigt_all_level`` /

@@ -143,6 +143,10 @@ int hpc_set_tensor_apply(hpc_ctx* ctx, int on);
 int hpc_launch_count(hpc_ctx* ctx, long long* count, int reset);
 /* The context's CUDA stream (cudaStream_t), for callers that time on it. */
 void* hpc_stream(hpc_ctx* ctx);
+/* No counterpart in the reference: the compute capability the library's device code was built for,
+ * as the CUDA runtime reports it for one of the library's kernels on the current device
+ * (major * 10 + minor: 100 for sm_100a).  HPC_ERR_NODEVICE without a device. */
+int hpc_binary_version(int* version);
 /* Kernel classes that can be timed with CUDA events on the context's stream. */
 enum hpc_kernel_class {
   HPC_KC_NONE = -1,
@@ -300,8 +304,11 @@ int hpc_image_material(hpc_ctx* ctx, const uint8_t* image, const int* voxel_n, i
  * code that must not trigger cudaMalloc's implicit synchronisation): the block partials live in a
  * fixed 1 MiB __device__ array that every device loading the library keeps until exit, so the call
  * allocates nothing.  n is limited to 134217728 (HPC_ERR_ARG beyond).  The first call on a device
- * looks up the scratch address once.  All calls share the scratch: calls that overlap on the GPU
- * race. */
+ * looks up the scratch address once; under lazy module loading (the CUDA 12 default) that lookup
+ * can load the library's device code and so allocate and synchronise: make one warm-up call (or any
+ * other call of this library on that device) before a region that must not allocate and before
+ * any stream capture.  The cached address does not survive cudaDeviceReset.  All calls share the
+ * scratch: calls that overlap on the GPU race. */
 int hpc_dmax_noalloc(const double* d, const double* d_old, long long n, double* out, void* stream);
 
 #ifdef __cplusplus

@@ -6,7 +6,7 @@ libhpcref.so, single-rank MPI stand-in) and driven through oracle/ref_harness.cp
 inputs; inputs and outputs are stored as compressed .npz fixtures.  The reference has no test
 vectors of its own, so these are its golden vectors.  Run from the repository root:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref REF=<reference source tree> && python tests/golden/make_golden.py
 """
 import os
 import sys
@@ -115,26 +115,36 @@ def solver_case(seed):
     return out
 
 
-def steps_case(name, steps, reference_schedule):
-    """Full staggered increments of a synthetic inclusion specimen, from the reference's own image
-    and CSV input path."""
+def steps_case(name, steps, reference_schedule, small_k=1e-5, mech_tol=1e-6, pf_tol=1e-12, keep=None):
+    """Full staggered increments of a synthetic specimen, from the reference's own image and CSV
+    input path; a pre-cracked workload gets its crack layer (H = H_crack on the crack elements, d = 1
+    on their nodes, H Voigt-averaged to every level) before the first increment.  Fields are kept
+    for the increments in `keep` (all by default); the step outputs for every increment.
+    Tolerances other than the reference's own (1e-6, 1e-12) run through the harness driver that
+    makes u_entire's / phase_field's calls with the threshold as a parameter."""
     import tempfile
     w = ms.make_workload(name)
     ref = B.RefOracle(w.maxlevel, w.element_nb, x0=w.x_start)
     with tempfile.TemporaryDirectory() as td:
         paths = ms.write_inputs(w, td)
         ref.input_total(td, paths["raw"], w.nodes, w.voxel_size)
-    out = {"name": name, "steps": steps}
+    out = {"name": name, "steps": steps, "small_k": small_k, "mech_tol": mech_tol, "pf_tol": pf_tol}
     L = w.maxlevel
+    if w.crack:
+        Hc, dc = ms.precrack_fields(w)
+        ref.set(B.H, L, Hc)
+        ref.set(B.D, L, dc)
+        ref.voigt_all_level(B.H)
     for f, key in ((B.BULK, "bulk"), (B.G, "g"), (B.GC, "gc")):
         out[key] = np.concatenate([ref.get(f, l) for l in range(L + 1)])
     kw = {} if reference_schedule else {"ut0": w.ut0, "dU": w.du}
     for t in range(steps):
-        o = ref.step(t, w.mg_u, w.mg_d, 1e-5, w.lc, w.voxel_size, **kw)
+        o = ref.step(t, w.mg_u, w.mg_d, small_k, w.lc, w.voxel_size, mech_tol=mech_tol, pf_tol=pf_tol, **kw)
         out[f"out_{t}"] = np.array(o)
-        out[f"u_{t}"] = ref.get(B.U, L)
-        out[f"d_{t}"] = ref.get(B.D, L)
-        out[f"H_{t}"] = ref.get(B.H, L)
+        if keep is None or t in keep:
+            out[f"u_{t}"] = ref.get(B.U, L)
+            out[f"d_{t}"] = ref.get(B.D, L)
+            out[f"H_{t}"] = ref.get(B.H, L)
     out["state"] = np.array(ref.state())
     ref.close()
     return out
@@ -142,16 +152,24 @@ def steps_case(name, steps, reference_schedule):
 
 def main():
     if not B.RefOracle.available():
-        raise SystemExit("oracle/_ref/libhpcref.so missing: make -C oracle ref")
+        raise SystemExit("oracle/_ref/libhpcref.so missing: make -C oracle ref REF=<reference source tree>")
     B.RefOracle._load().ref_set_threads(os.cpu_count() or 1)
-    cases = {
-        "ops_iso": ops_case(2, (2, 2, 2), (-3.0, 1.5, -7.0), 11),
-        "ops_xwide": ops_case(1, (4, 3, 2), (0.0, 0.0, 0.0), 12),
-        "ops_ywide": ops_case(1, (2, 7, 3), (-1.0, -1.0, -1.0), 13),
-        "solver": solver_case(21),
-        "steps17": steps_case("small17", 4, reference_schedule=False),
-        "steps17_ue": steps_case("small17", 2, reference_schedule=True),
+    builders = {
+        "ops_iso": lambda: ops_case(2, (2, 2, 2), (-3.0, 1.5, -7.0), 11),
+        "ops_xwide": lambda: ops_case(1, (4, 3, 2), (0.0, 0.0, 0.0), 12),
+        "ops_ywide": lambda: ops_case(1, (2, 7, 3), (-1.0, -1.0, -1.0), 13),
+        "solver": lambda: solver_case(21),
+        "steps17": lambda: steps_case("small17", 4, reference_schedule=False),
+        "steps17_ue": lambda: steps_case("small17", 2, reference_schedule=True),
+        # the benchmarked specimen's recipe (three phases with pores, pre-crack) at 33^3: at the
+        # benchmark's tolerance |r|/|f| <= 1e-8 (squared 1e-16) with fields of the first and last
+        # increments, and at the reference's own thresholds (step outputs only)
+        "crack33": lambda: steps_case("crack33", 3, reference_schedule=False, small_k=1e-6, mech_tol=1e-16,
+                                      pf_tol=1e-16, keep=(0, 2)),
+        "crack33_reftol": lambda: steps_case("crack33", 3, reference_schedule=False, small_k=1e-6, keep=()),
     }
+    only = sys.argv[1:]  # optional subset of fixture names
+    cases = {name: build() for name, build in builders.items() if not only or name in only}
     for name, data in cases.items():
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **{k: np.asarray(v) for k, v in data.items()})

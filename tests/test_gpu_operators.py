@@ -148,3 +148,12 @@ def test_initial_crack(pair):
         for impl in (gpu, orc):
             impl.initial_crack(7.5, l)
         assert np.array_equal(gpu.get(H, l), orc.get(H, l))
+
+
+def test_binary_version_is_sm100():
+    """The runtime reports the library's kernels as built for compute capability 10.0 (sm_100a)."""
+    import ctypes as C
+    from hpcrack_b200 import lib as L
+    v = C.c_int(0)
+    L.check("hpc_binary_version", L.load().hpc_binary_version(C.byref(v)))
+    assert v.value == 100, v.value

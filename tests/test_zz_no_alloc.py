@@ -47,6 +47,22 @@ def test_noalloc_dmax_matches_context_entry_points():
         torch.cuda.synchronize()
         got = out.cpu().numpy()
         assert got[0] == want_dd and got[1] == want_dm, (call, got, want_dd, want_dm)
+    # a size of several hundred blocks with a ragged last block: the last block's combine loop
+    # strides over more than 32 partials; the maxima are exact, so numpy gives the same values
+    n_big = (1 << 20) + 12345
+    d = rng.uniform(-0.5, 1.0, n_big)
+    d_old = d - rng.uniform(-0.2, 0.3, n_big)
+    d[n_big - 3] = 2.5  # the maximum sits in the partial last block
+    td = torch.tensor(d, device="cuda")
+    to = torch.tensor(d_old, device="cuda")
+    for call in range(2):
+        out.zero_()
+        rc = lib.hpc_dmax_noalloc(C.c_void_p(td.data_ptr()), C.c_void_p(to.data_ptr()), n_big,
+                                  C.c_void_p(out.data_ptr()), C.c_void_p(stream))
+        L.check("hpc_dmax_noalloc", rc)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert got[0] == max(0.0, float(np.max(d - d_old))) and got[1] == max(0.0, float(np.max(d))), (call, got)
     # sizes beyond the fixed scratch are refused with a clear error, before any launch
     rc = lib.hpc_dmax_noalloc(C.c_void_p(td.data_ptr()), C.c_void_p(to.data_ptr()), 134217729,
                               C.c_void_p(out.data_ptr()), C.c_void_p(stream))
