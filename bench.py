@@ -41,6 +41,11 @@ FALLBACK_HBM_GBS = 6650.0
 # instructions, its bound, for bytes).
 APPLY_BYTES_PER_NODE = 74
 PCG_APPLY_BYTES_PER_NODE = 176
+# With the direction update p = M^-1 r + beta p fused into the apply (--fused-direction), the kernel also
+# reads z = M^-1 r and the previous direction and writes the new one: +72 algorithmic bytes per node
+# (the compulsory traffic of that vector update), +48 on top of what the unfused apply reads.
+FUSED_DIR_BYTES_PER_NODE = 72
+FUSED_DIR_EXTRA_READ_PER_NODE = 48
 # ncu counters of the FP64 apply (one capture of the 193^3 level, the same kernel the bench times):
 # FP64 pipe active 60.7 % of active cycles, issue active 56.1 %, top stall "wait" (fixed-latency
 # dependencies) 1.36 per issued instruction.
@@ -64,6 +69,9 @@ def parse_args():
     ap.add_argument("--mech-solver", choices=("fas", "fcg", "mixed"), default="fas",
                     help="fas: the reference's FAS V-cycles (plain form); fcg: flexible PCG preconditioned by one "
                          "FP64 V-cycle per iteration; mixed: the precision form (FP32 V-cycle, FP64 outer PCG)")
+    ap.add_argument("--fused-direction", action="store_true",
+                    help="finest PCG direction update inside the operator apply (hpc_set_fused_direction 1) "
+                         "instead of a pass of its own")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-timing", action="store_true")
@@ -401,6 +409,8 @@ def run_b200(args, rank, world, local):
     hier = load_specimen(w, local)
     if args.autotune:
         hier.set_autotune(True)
+    fused_dir = args.fused_direction
+    hier.set_fused_direction(fused_dir)
     stream = torch.cuda.ExternalStream(hier.stream())
 
     solver = MECH_SOLVERS[args.mech_solver]
@@ -450,19 +460,26 @@ def run_b200(args, rank, world, local):
     # (PCG_APPLY_BYTES_PER_NODE algorithmic bytes per finest node).
     roofline = None
     if kn > 0:
-        achieved = N * APPLY_BYTES_PER_NODE / (kms / kn / 1e3) / 1e9
-        achieved_read = N * PCG_APPLY_BYTES_PER_NODE / (kms / kn / 1e3) / 1e9
+        alg = APPLY_BYTES_PER_NODE + (FUSED_DIR_BYTES_PER_NODE if fused_dir else 0)
+        read = PCG_APPLY_BYTES_PER_NODE + (FUSED_DIR_EXTRA_READ_PER_NODE if fused_dir else 0)
+        achieved = N * alg / (kms / kn / 1e3) / 1e9
+        achieved_read = N * read / (kms / kn / 1e3) / 1e9
         peak, src = peaks()
-        roofline = {"bound": "hbm", "kernel": "mech_kernel<finest, PCG, Gauss-point moduli> (w = K(d) p, (p, w))",
+        kname = ("mech_kernel<finest, PCG + direction update, Gauss-point moduli> (p = M^-1 r + beta p, w = K(d) p, "
+                 "(p, w))" if fused_dir else "mech_kernel<finest, PCG, Gauss-point moduli> (w = K(d) p, (p, w))")
+        basis = "algorithmic: u 24 + bulK,G,d 24 + regime 2 + out 24 B per finest node"
+        if fused_dir:
+            basis += " + direction update z 24 + p_old 24 + p 24"
+        roofline = {"bound": "hbm", "kernel": kname,
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "peak_source": src, "bytes_per_node": APPLY_BYTES_PER_NODE,
-                    "bytes_basis": "algorithmic: u 24 + bulK,G,d 24 + regime 2 + out 24 B per finest node",
+                    "peak_source": src, "bytes_per_node": alg, "bytes_basis": basis,
                     "traffic": PCG_APPLY_TRAFFIC_PER_NODE * N,
                     "traffic_note": "bytes per launch: ncu dram bytes per node of the 193^3 capture x nodes; above "
-                                    "the 74 B/node because the kernel reads precomputed Gauss-point moduli",
-                    "read_layout": {"bytes_per_node": PCG_APPLY_BYTES_PER_NODE, "achieved": achieved_read,
+                                    "the algorithmic bytes because the kernel reads precomputed Gauss-point moduli",
+                    "read_layout": {"bytes_per_node": read, "achieved": achieved_read,
                                     "frac": achieved_read / peak,
-                                    "what": "p, w and the precomputed Gauss-point moduli the kernel reads"},
+                                    "what": "the vectors and the precomputed Gauss-point moduli the kernel reads "
+                                            "and writes"},
                     "fp64_pipe_active_ncu": APPLY_FP64_PIPE_ACTIVE,
                     "limiter": "FP64 pipe (dependent FP64 latency), not HBM",
                     "launches": kn, "avg_launch_ms": kms / kn}

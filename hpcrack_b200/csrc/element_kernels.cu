@@ -139,6 +139,9 @@ struct MechKT {
   const T* invM;
   const T* rf;
   const T* gpm;  // finest level, precomputed Gauss-point moduli: K - 2G/3 at [g * n + e], G at [(8 + g) * n + e]
+  T* zout;       // RESIDUAL: z = M^-1 r written here when not null
+  T* pnew;       // PCGDIR: the new direction, written by each node's owner
+  int s_bnum, s_bden, first;  // PCGDIR: beta = scal[s_bnum] / scal[s_bden], 0 when first
   RedTarget red;
   double* err;   // tensor-core kernel: set to 1 when a bounded wait ran out
 };
@@ -230,14 +233,20 @@ __device__ __forceinline__ void assemble_row(const MechKT<T>& k, const Stream<NF
           if (k.red.slot[0] >= 0) red0 = fma((double)fv, (double)fv, red0);  // sums nobody reads are skipped
           const T rv = fix[m] ? T(0) : fv - tot[m];
           k.out[n + m * N] = rv;
-          if (k.invM) red1 = fma((double)rv, (double)(rv * k.invM[n + m * N]), red1);
+          if (k.invM) {
+            const T zv = rv * k.invM[n + m * N];
+            if (k.zout) k.zout[n + m * N] = zv;
+            red1 = fma((double)rv, (double)zv, red1);
+          }
           if (k.red.slot[2] >= 0) red2 = fma((double)rv, (double)rv, red2);
         }
-      } else if (EPI == EPI_PCG) {  // w = K p, (p, w)
+      } else if (EPI == EPI_PCG || EPI == EPI_PCGDIR) {  // w = K p, (p, w); PCGDIR: the owner writes p
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
+          const T pv = st.at(si - 1, m, 0, lane);
           k.out[n + m * N] = tot[m];
-          red0 = fma((double)st.at(si - 1, m, 0, lane), (double)tot[m], red0);
+          if (EPI == EPI_PCGDIR) k.pnew[n + m * N] = pv;
+          red0 = fma((double)pv, (double)tot[m], red0);
         }
       } else if (EPI == EPI_FAS) {
         // coarsen_f_standard_routine (multigrid_intergrid.cpp:124-342) fused with the coarse apply
@@ -262,10 +271,16 @@ __device__ __forceinline__ void assemble_row(const MechKT<T>& k, const Stream<NF
 // T = double: the plain form; T = float: the precision form's V-cycle (reductions stay FP64).
 // GPM: the finest level's Gauss-point moduli come precomputed (gp_material_kernel) instead of being
 // interpolated from the staged nodal K, G, d in every apply.
+// EPI_PCGDIR (FINEST && GPM): the staged fields are z = M^-1 r (0..2) and the previous direction
+// (3..5); each lane turns its column of a row that has landed into p = z + beta p_old in place, before
+// any lane reads the row, so the element math sees p.  (A call's first iteration passes z as p_old
+// with beta = 0: fma(0, z, z) = z.)
 template <typename T, bool FINEST, int EPI, bool DIAG, bool ISO, bool GPM = false>
 __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
   constexpr int NU = DIAG ? 0 : 3;
-  constexpr int NF = NU + (FINEST ? (GPM ? 0 : 3) : 2);
+  constexpr bool PDIR = EPI == EPI_PCGDIR;
+  static_assert(!PDIR || (FINEST && GPM && !DIAG), "the fused direction update runs on precomputed moduli");
+  constexpr int NF = PDIR ? 6 : NU + (FINEST ? (GPM ? 0 : 3) : 2);
   extern __shared__ __align__(16) unsigned char mech_smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   T* ring = reinterpret_cast<T*>(mech_smem) + (size_t)wib * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32);
@@ -273,6 +288,8 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
   const SFt<T> s = make_sf<T>(k.g);
   double red0 = 0.0, red1 = 0.0, red2 = 0.0;
   const long long nwarps_total = (long long)gridDim.x * kWarps;
+  T beta = T(0);
+  if (PDIR && !k.first) beta = (T)(k.red.scal[k.s_bnum] / k.red.scal[k.s_bden]);
   const T* fptr[NF];
 #pragma unroll
   for (int f = 0; f < NF; ++f) fptr[f] = k.fields[f];
@@ -295,6 +312,17 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
       st.issue(si + 2, lane);
       cp_async_wait2();
       __syncwarp();
+      if constexpr (PDIR) {  // p = z + beta p_old on this lane's column of the row that just landed
+        T* slot = ring + (size_t)(si & (kRing - 1)) * NF * 2 * kRowW;
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            T* zp = slot + (m * 2 + c) * kRowW + lane;
+            *zp = fma(beta, slot[((3 + m) * 2 + c) * kRowW + lane], *zp);
+          }
+        __syncwarp();
+      }
       const int li = si / rows, r = si - li * rows;
       const int kk = z0 - 1 + li;
       if (r == 0) {
@@ -374,7 +402,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
       __syncwarp();
     }
   }
-  if (EPI == EPI_RESIDUAL || EPI == EPI_PCG) {
+  if (EPI == EPI_RESIDUAL || EPI == EPI_PCG || EPI == EPI_PCGDIR) {
     double v[3] = {red0, red1, red2};
     grid_reduce<3>(v, k.red);
   }
@@ -887,9 +915,21 @@ inline bool iso(const LevelGeo& g) { return g.hx == g.hy && g.hy == g.hz; }
 
 template <bool F, int E, bool D, typename T = double>
 static int run_mech(hpc_ctx* c, const MechKT<T>& k) {
-  const int cls = (F && E == EPI_PCG && !D) ? (sizeof(T) == 8 ? HPC_KC_MECH_PCG_FINEST : HPC_KC_MECH32_PCG_FINEST)
-                                             : HPC_KC_NONE;
-  if constexpr (F && !D) {
+  const int cls = (F && (E == EPI_PCG || E == EPI_PCGDIR) && !D)
+                      ? (sizeof(T) == 8 ? HPC_KC_MECH_PCG_FINEST : HPC_KC_MECH32_PCG_FINEST)
+                      : HPC_KC_NONE;
+  if constexpr (E == EPI_PCGDIR) {
+    static_assert(F && !D, "fused direction update: finest PCG apply only");
+    if (!k.gpm) {
+      set_error("fused direction update without precomputed Gauss-point moduli");
+      return HPC_ERR_ARG;
+    }
+    constexpr int NF = 6;  // z and the previous direction
+    const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
+    if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true, true>, k, smem, cls);
+    return launch_strips(c, mech_kernel<T, F, E, D, false, true>, k, smem, cls);
+  }
+  if constexpr (F && !D && E != EPI_PCGDIR) {
     if (k.gpm) {  // precomputed Gauss-point moduli: only u is staged
       constexpr int NF = 3;
       const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
@@ -897,12 +937,15 @@ static int run_mech(hpc_ctx* c, const MechKT<T>& k) {
       return launch_strips(c, mech_kernel<T, F, E, D, false, true>, k, smem, cls);
     }
   }
-  constexpr int NF = (D ? 0 : 3) + (F ? 3 : 2);
-  const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
-  if constexpr (!D) {
-    if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true>, k, smem, cls);
+  if constexpr (E != EPI_PCGDIR) {
+    constexpr int NF = (D ? 0 : 3) + (F ? 3 : 2);
+    const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
+    if constexpr (!D) {
+      if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true>, k, smem, cls);
+    }
+    return launch_strips(c, mech_kernel<T, F, E, D, false>, k, smem, cls);
   }
-  return launch_strips(c, mech_kernel<T, F, E, D, false>, k, smem, cls);
+  return HPC_ERR_ARG;
 }
 
 static void mech_fields(hpc_ctx* c, int level, bool finest, bool diag, const double* src, MechK& k) {
@@ -936,8 +979,23 @@ int launch_mech(hpc_ctx* c, const MechCall& m) {
   k.rf = m.rf;
   k.gpm = (m.finest && c->gpm_active) ? c->F[m.level].gpm : nullptr;
   k.red = make_red(c, m.s_out0, m.s_out1, m.s_out2);
+  k.zout = m.zout;
+  if (m.epi == EPI_PCGDIR) {
+    const long long n = c->L[m.level].n;
+    for (int q = 0; q < 3; ++q) k.fields[3 + q] = (m.first ? m.src : m.pold) + (long long)q * n;
+    k.pnew = m.pnew;
+    k.s_bnum = m.s_bnum;
+    k.s_bden = m.s_bden;
+    k.first = m.first ? 1 : 0;
+  }
   const bool f = m.finest;
   switch (m.epi) {
+    case EPI_PCGDIR:
+      if (!f) {
+        set_error("fused direction update on a coarse level");
+        return HPC_ERR_ARG;
+      }
+      return run_mech<true, EPI_PCGDIR, false>(c, k);
     case EPI_PLAIN: return f ? run_mech<true, EPI_PLAIN, false>(c, k) : run_mech<false, EPI_PLAIN, false>(c, k);
     case EPI_RESIDUAL:
       return f ? run_mech<true, EPI_RESIDUAL, false>(c, k) : run_mech<false, EPI_RESIDUAL, false>(c, k);

@@ -104,7 +104,7 @@ static bool geometry_ok(const hpc_geometry* g) {
 // Number of doubles per level allocated for a level with n padded slots.
 constexpr int kScalarFieldsPerLevel = 10;  // bulK G gc d H fd Ke Ge R dold
 constexpr int kVectorFieldsPerLevel = 4;   // u fu ru uold
-constexpr int kWork3 = 4, kWork1 = 4;      // preMu p w tmp3 / preMd pd wd tmp1
+constexpr int kWork3 = 4, kWork1 = 4;      // preMu p w z / preMd pd wd tmp1
 static size_t level_bytes(long long n) {
   return (size_t)n * sizeof(double) * (kScalarFieldsPerLevel + 3 * kVectorFieldsPerLevel + 3 * kWork3 + kWork1) +
          (size_t)n;  // choice
@@ -235,7 +235,39 @@ static int pcg_u_dev(hpc_ctx* c, int l, double small_k, double Ut, int nb, int t
   m.s_out0 = m.set_fnorm ? S_FNORM : -1;
   m.s_out1 = slot_rz(0);
   m.s_out2 = S_RNORM;
+  // Finest level with the precomputed Gauss-point moduli: the direction update p = M^-1 r + beta p
+  // happens inside the apply's staging (EPI_PCGDIR) from z = M^-1 r, which the residual and the
+  // updates write; the directions alternate between two buffers, since neighbouring strips still read
+  // the old direction while a node's owner writes the new one.  Same products and fma as the
+  // separate pass, so the same bits.
+  const bool fuse = m.finest && c->fused_dir && c->gpm_active && F.p2 && nb > 0;
+  if (fuse) m.zout = F.z;
   if ((rc = launch_mech(c, m))) return rc;
+  if (fuse) {
+    double* dirs[2] = {F.p, F.p2};
+    for (int it = 0; it < nb; ++it) {
+      MechCall q{};
+      q.level = l;
+      q.finest = true;
+      q.epi = EPI_PCGDIR;
+      q.src = F.z;
+      q.pold = dirs[it & 1];
+      q.pnew = dirs[(it + 1) & 1];
+      q.first = it == 0;
+      q.s_bnum = slot_rz(it);
+      q.s_bden = slot_rz(it - 1);
+      q.out = F.w;
+      q.small_k = small_k;
+      q.s_out0 = slot_pw(it);
+      q.s_out1 = q.s_out2 = -1;
+      if ((rc = launch_mech(c, q))) return rc;
+      // z for the next iteration's apply (none after the last: the next call starts from a residual)
+      if ((rc = launch_mech_update_on(c, l, F.u, F.ru, q.pnew, F.w, F.preMu, slot_rz(it), slot_pw(it),
+                                      slot_rz(it + 1), slot_rn(it), it + 1 < nb ? F.z : nullptr)))
+        return rc;
+    }
+    return HPC_OK;
+  }
   for (int it = 0; it < nb; ++it) {
     if ((rc = launch_dir_update(c, l, 3, F.ru, F.preMu, F.p, it == 0, slot_rz(it), slot_rz(it - 1)))) return rc;
     MechCall q{};
@@ -369,7 +401,9 @@ static bool same_mg(const hpc_mg& a, const hpc_mg& b) {
 // parameters differ from the cached ones (the kernels' first use must already have happened,
 // `allow_capture`), replayed afterwards.  Kernel launches are counted per replay.  A graph is keyed
 // by its parameters and by `flags`, the context's kernel choices baked into its launches.
-static int graph_flags(const hpc_ctx* c) { return c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active; }
+static int graph_flags(const hpc_ctx* c) {
+  return c->fused_dir * 8 + c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active;
+}
 template <class Body>
 static int run_graphed(hpc_ctx* c, hpc_ctx::CoarseGraph& g, const hpc_mg& mg, double a, double b, bool allow_capture,
                        Body body, int flags) {
@@ -460,6 +494,11 @@ static int gp_material(hpc_ctx* c, double small_k) {
     const size_t bytes = sizeof(double) * 16 * (size_t)c->L[c->maxlevel].n;
     HPC_CUDA(cudaMalloc((void**)&F.gpm, bytes));
     HPC_CUDA(cudaMemsetAsync(F.gpm, 0, bytes, c->stream));  // non-element slots stay zero
+  }
+  if (!F.p2) {  // the second direction buffer of the fused direction update (same first use)
+    const size_t bytes = sizeof(double) * 3 * (size_t)c->L[c->maxlevel].n;
+    HPC_CUDA(cudaMalloc((void**)&F.p2, bytes));
+    HPC_CUDA(cudaMemsetAsync(F.p2, 0, bytes, c->stream));  // padding slots stay zero
   }
   int rc = launch_gp_material(c, small_k);
   if (rc) return rc;
@@ -915,9 +954,10 @@ int hpc_footprint(const hpc_geometry* geo, size_t* bytes) {
   const size_t nf = (size_t)f.px * f.ny * f.nz;
   total += nf * sizeof(double);  // d_old
   total += sizeof(double) * (kScalarPool + 3 * 8192) + 64;
-  // allocated on first use: Gauss-point moduli (16 n), flexible-PCG vectors (5 x 3n), the FP32
-  // mirror of every level (7 x 3n + material) with its Gauss-point moduli, the checkpoint (6 dense)
-  total += nf * sizeof(double) * (16 + 15);
+  // allocated on first use: Gauss-point moduli (16 n) with the second PCG direction (3n),
+  // flexible-PCG vectors (5 x 3n), the FP32 mirror of every level (7 x 3n + material) with its
+  // Gauss-point moduli, the checkpoint (6 dense)
+  total += nf * sizeof(double) * (16 + 3 + 15);
   for (int l = 0; l <= geo->maxlevel; ++l) {
     const size_t n = (size_t)lv[l].px * lv[l].ny * lv[l].nz;
     total += n * sizeof(float) * (21 + (l == geo->maxlevel ? 3 + 16 : 2));
@@ -948,6 +988,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   c->choice_quirk = 1;
   c->use_graphs = 1;
   c->fused_coarsest = 1;
+  c->fused_dir = 0;  // measured slower than the separate pass on B200 (hpc_set_fused_direction)
   c->timing_class = HPC_KC_NONE;
   HostLevel lv[kMaxLevels];
   host_geometry(*geo, c->box, lv);
@@ -1007,7 +1048,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
     const long long n = c->L[l].n;
     LevelFields& F = c->F[l];
     double** scal[] = {&F.bulK, &F.G, &F.gc, &F.d, &F.H, &F.fd, &F.Ke, &F.Ge, &F.R, &F.dold, &F.preMd, &F.pd, &F.wd, &F.tmp1};
-    double** vec[] = {&F.u, &F.fu, &F.ru, &F.uold, &F.preMu, &F.p, &F.w, &F.tmp3};
+    double** vec[] = {&F.u, &F.fu, &F.ru, &F.uold, &F.preMu, &F.p, &F.w, &F.z};
     for (double** p : scal) {
       cudaError_t ae = cudaMalloc((void**)p, sizeof(double) * n);
       if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMalloc(level field)"));
@@ -1054,7 +1095,7 @@ int hpc_destroy(hpc_ctx* c) {
   for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
     LevelFields& F = c->F[l];
     void* ptrs[] = {F.bulK, F.G, F.gc, F.d, F.H, F.fd, F.Ke, F.Ge, F.R, F.dold, F.preMd, F.pd, F.wd, F.tmp1,
-                    F.u, F.fu, F.ru, F.uold, F.preMu, F.p, F.w, F.tmp3, F.choice, F.gpm};
+                    F.u, F.fu, F.ru, F.uold, F.preMu, F.p, F.w, F.z, F.p2, F.choice, F.gpm};
     for (void* p : ptrs)
       if (p) cudaFree(p);
   }
@@ -1117,6 +1158,12 @@ int hpc_set_tensor_apply(hpc_ctx* c, int on) {
 int hpc_set_fused_coarsest(hpc_ctx* c, int on) {
   if (!c) return arg_fail("null context");
   c->fused_coarsest = on != 0;
+  return HPC_OK;
+}
+
+int hpc_set_fused_direction(hpc_ctx* c, int on) {
+  if (!c) return arg_fail("null context");
+  c->fused_dir = on != 0;
   return HPC_OK;
 }
 

@@ -37,7 +37,8 @@ struct LevelFields {
   double *u, *fu, *ru, *uold;  // 3n each; component c at +c*n
   int8_t* choice;
   // work arrays
-  double *preMu, *p, *w, *tmp3;  // 3n; preMu holds the inverse diagonal while a solve runs
+  double *preMu, *p, *w, *z;     // 3n; preMu holds the inverse diagonal while a solve runs; z = M^-1 r
+  double* p2;                     // finest level: second PCG direction of the fused direction update (first use)
   double *preMd, *pd, *wd, *tmp1;  // n;  preMd likewise
   uint8_t* bc_host_copy;           // host copies of the axis flags (nx+ny+nz bytes)
   double* gpm;  // finest level: Gauss-point moduli of the running mechanical solve, 16n (first use)
@@ -118,6 +119,7 @@ struct hpc_ctx {
   int tc_apply;        // precision form: element contraction on the tensor cores (hpc_set_tensor_apply)
   int fused_coarsest;  // coarse-level pcg_u in one block when the level fits (hpc_set_fused_coarsest)
   int gpm_active;      // finest applies read F[maxlevel].gpm (set while a mechanical solve runs)
+  int fused_dir;       // finest pcg_u forms p = M^-1 r + beta p inside the apply (hpc_set_fused_direction)
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
@@ -181,7 +183,10 @@ int vtk_release(hpc_ctx* c);
 
 // ---------------------------------------------------------------- kernel launchers
 // Element operators (element_kernels.cu).  `src` is a 3n (mech) or n (pf) vector on level L.
-enum MechEpi { EPI_PLAIN = 0, EPI_RESIDUAL = 1, EPI_PCG = 2, EPI_FAS = 3, EPI_REACTION = 4 };
+// EPI_PCGDIR: the PCG apply with the direction update in its staging: p = z + beta p_old formed from
+// the staged z = M^-1 r and p_old, w = K p, (p, w), p written by the node's owner (finest level,
+// precomputed Gauss-point moduli).
+enum MechEpi { EPI_PLAIN = 0, EPI_RESIDUAL = 1, EPI_PCG = 2, EPI_FAS = 3, EPI_REACTION = 4, EPI_PCGDIR = 5 };
 
 struct MechCall {
   int level;
@@ -194,6 +199,12 @@ struct MechCall {
   double* fu;
   bool set_fnorm;     // t == 0 on the finest level (mechanical_pcg.cpp:252-258)
   const double* invM; // RESIDUAL: inverse diagonal for rz = sum r^2 invM (null: no rz)
+  double* zout;       // RESIDUAL: z = M^-1 r written here when not null
+  // PCGDIR: src = z; p = first ? z : z + beta p_old with beta = scal[s_bnum] / scal[s_bden]
+  const double* pold;
+  double* pnew;
+  int s_bnum, s_bden;
+  bool first;
   // FAS: fc = K_c u_c + full-weighting(rf)
   const double* rf;
   int fine_level;
@@ -254,8 +265,9 @@ int launch_pf_diag(hpc_ctx* c, int level, double lc, double* out);
 // nodes; scal[s_rz_next] = sum r^2/preM; scal[s_rn] = sum r^2.
 int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
 // Same on explicit arrays: x += alpha p, r -= alpha w (Dirichlet rows zero), alpha = scal[s_num]/scal[s_den].
+// zout (optional): z = M^-1 r of the updated residual, for a following fused direction update.
 int launch_mech_update_on(hpc_ctx* c, int level, double* x, double* r, const double* p, const double* w,
-                          const double* invM, int s_num, int s_den, int s_rz_next, int s_rn);
+                          const double* invM, int s_num, int s_den, int s_rz_next, int s_rn, double* zout = nullptr);
 // sums (a, b) and (a, c) over a 3n vector of a level into scal[s0], scal[s1] (c may be null)
 int launch_dot2(hpc_ctx* c, int level, const double* a, const double* b, const double* cv, int s0, int s1);
 int launch_dot2(hpc_ctx* c, int level, const float* a, const double* b, const double* cv, int s0, int s1);

@@ -155,6 +155,11 @@ class Hierarchy:
         """Coarsest-level pcg_u in one thread block (default) or as per-iteration kernels."""
         self._c("hpc_set_fused_coarsest", int(bool(on)))
 
+    def set_fused_direction(self, on: bool):
+        """hpc_set_fused_direction: the finest PCG direction update inside the operator apply (1) or
+        as a pass of its own (0, default, faster on B200); the same bits either way."""
+        self._c("hpc_set_fused_direction", int(bool(on)))
+
     def set_autotune(self, on: bool):
         """Measure strip shapes on first use of each kernel and level size (see hpc_set_autotune)."""
         self._c("hpc_set_autotune", int(bool(on)))

@@ -132,6 +132,12 @@ int hpc_tuned_shapes(int* out5, int cap, int* count);
  * shared memory (up to about 10^3 nodes); 0 uses the per-iteration kernels.  The two differ only in
  * the order of the same sums. */
 int hpc_set_fused_coarsest(hpc_ctx* ctx, int on);
+/* No counterpart in the reference: 1 forms the PCG direction p = M^-1 r + beta p of the
+ * finest-level mechanical smoother (mechanical_pcg.cpp:274-292) inside the next operator apply's
+ * staging instead of in a pass of its own, while the Gauss-point moduli of a mechanical solve are
+ * in use; 0 (default) keeps the separate pass.  Both compute the same products and fma: the same
+ * bits.  On B200 the fused apply (twice the staged rows) costs more than the pass it saves. */
+int hpc_set_fused_direction(hpc_ctx* ctx, int on);
 /* No counterpart in the reference: 1 runs the element operator of the precision form's FP32 V-cycle
  * (mech_solver HPC_MECH_MIXED) on the tensor cores - strains and element forces as two TF32 GEMMs
  * per 128 elements (tcgen05, accumulators in tensor memory), Hooke's law per Gauss point on the
