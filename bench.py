@@ -41,11 +41,6 @@ FALLBACK_HBM_GBS = 6650.0
 # instructions, its bound, for bytes).
 APPLY_BYTES_PER_NODE = 74
 PCG_APPLY_BYTES_PER_NODE = 176
-# With the direction update p = M^-1 r + beta p fused into the apply (--fused-direction), the kernel also
-# reads z = M^-1 r and the previous direction and writes the new one: +72 algorithmic bytes per node
-# (the compulsory traffic of that vector update), +48 on top of what the unfused apply reads.
-FUSED_DIR_BYTES_PER_NODE = 72
-FUSED_DIR_EXTRA_READ_PER_NODE = 48
 # ncu counters of the FP64 apply (one capture of the 193^3 level, the same kernel the bench times):
 # FP64 pipe active 60.7 % of active cycles, issue active 56.1 %, top stall "wait" (fixed-latency
 # dependencies) 1.36 per issued instruction.
@@ -69,9 +64,6 @@ def parse_args():
     ap.add_argument("--mech-solver", choices=("fas", "fcg", "mixed"), default="fas",
                     help="fas: the reference's FAS V-cycles (plain form); fcg: flexible PCG preconditioned by one "
                          "FP64 V-cycle per iteration; mixed: the precision form (FP32 V-cycle, FP64 outer PCG)")
-    ap.add_argument("--fused-direction", action="store_true",
-                    help="finest PCG direction update inside the operator apply (hpc_set_fused_direction 1) "
-                         "instead of a pass of its own")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-timing", action="store_true")
@@ -102,6 +94,10 @@ def parse_args():
     ap.add_argument("--requests", type=int, default=24, help="requests in a --serve sample")
     ap.add_argument("--increments", type=int, default=0, help="increments per request (default 10 serve, 5 batch)")
     ap.add_argument("--slots", type=int, default=8, help="concurrent requests on the GPU")
+    ap.add_argument("--engine", choices=("batch", "threads"), default="batch",
+                    help="serving / batched forms: batch = one engine thread advancing every active request by one "
+                         "increment per batched call (hpc_batch_step: device-driven solve loops, one graph launch "
+                         "per solve phase for all requests); threads = one worker thread and stream per slot")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     ap.add_argument("--sizes", default="", help="serve: comma list of cubic sizes to draw from (default: the mix)")
     return ap.parse_args()
@@ -131,8 +127,9 @@ def run_serving(args, local):
         v = tuple(int(x) for x in args.mg_u.split(","))
         for q in reqs:
             q.workload.mg_u = v + (q.workload.mg_u[4],)
-    srv = sv.SolveServer(budget, args.slots, solver_factory=sv.default_factory(local),
-                         mech_solver=MECH_SOLVERS[args.mech_solver], precision_mg=not args.mg_u)
+    server = sv.BatchServer if args.engine == "batch" else sv.SolveServer
+    srv = server(budget, args.slots, solver_factory=sv.default_factory(local),
+                 mech_solver=MECH_SOLVERS[args.mech_solver], precision_mg=not args.mg_u)
     from hpcrack_b200.solver import precision_mg
     mg_used = reqs[0].workload.mg_u
     if args.mech_solver != "fas" and not args.mg_u:
@@ -147,12 +144,13 @@ def run_serving(args, local):
         nx, ny, nz = q.workload.nodes
         dof_iters += sum(3.0 * nx * ny * nz * o[6] + nx * ny * nz * o[7] for o in r.outputs)
     line = {"metric": metric, "value": st["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
-            "dtype": "f64", "data": "synthetic", "config": {"workload": form, "slots": args.slots,
+            "dtype": "f64", "data": "synthetic", "config": {"workload": form, "slots": args.slots, "engine": args.engine,
                                                             "hbm_budget_gb": args.hbm_budget_gb,
                                                             "mech_solver": args.mech_solver,
                                                             "mg_u": mg_used if isinstance(mg_used, str)
                                                             else list(mg_used)},
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "wall_s": wall,
+            "batched_calls": getattr(srv, "rounds", None),
             "mdof_iter_per_s": dof_iters / wall / 1e6, "peak_active": srv.peak_active,
             "peak_hbm_gb": srv.peak_used / (1 << 30)}
     print(json.dumps(line), flush=True)
@@ -409,8 +407,6 @@ def run_b200(args, rank, world, local):
     hier = load_specimen(w, local)
     if args.autotune:
         hier.set_autotune(True)
-    fused_dir = args.fused_direction
-    hier.set_fused_direction(fused_dir)
     stream = torch.cuda.ExternalStream(hier.stream())
 
     solver = MECH_SOLVERS[args.mech_solver]
@@ -460,16 +456,13 @@ def run_b200(args, rank, world, local):
     # (PCG_APPLY_BYTES_PER_NODE algorithmic bytes per finest node).
     roofline = None
     if kn > 0:
-        alg = APPLY_BYTES_PER_NODE + (FUSED_DIR_BYTES_PER_NODE if fused_dir else 0)
-        read = PCG_APPLY_BYTES_PER_NODE + (FUSED_DIR_EXTRA_READ_PER_NODE if fused_dir else 0)
+        alg = APPLY_BYTES_PER_NODE
+        read = PCG_APPLY_BYTES_PER_NODE
         achieved = N * alg / (kms / kn / 1e3) / 1e9
         achieved_read = N * read / (kms / kn / 1e3) / 1e9
         peak, src = peaks()
-        kname = ("mech_kernel<finest, PCG + direction update, Gauss-point moduli> (p = M^-1 r + beta p, w = K(d) p, "
-                 "(p, w))" if fused_dir else "mech_kernel<finest, PCG, Gauss-point moduli> (w = K(d) p, (p, w))")
+        kname = "mech_kernel<finest, PCG, Gauss-point moduli> (w = K(d) p, (p, w))"
         basis = "algorithmic: u 24 + bulK,G,d 24 + regime 2 + out 24 B per finest node"
-        if fused_dir:
-            basis += " + direction update z 24 + p_old 24 + p 24"
         roofline = {"bound": "hbm", "kernel": kname,
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "peak_source": src, "bytes_per_node": alg, "bytes_basis": basis,

@@ -25,7 +25,9 @@
 namespace hpc {
 
 constexpr int kWarps = 4;    // warps per block
-constexpr int kWY = 8;       // largest strip height in element rows (wy - 1 output node rows)
+// Largest strip height in element rows (wy - 1 output node rows).  16-row strips (half the y
+// recomputation) ran the 257^3 FP64 apply at 1.33 ms against 1.07 ms with 8 rows: measured and dropped.
+constexpr int kWY = 8;
 constexpr int kOX = 30;      // output nodes per strip in x (lanes 1..30)
 constexpr int kRowW = 33;    // staged row width (32 lanes + the x+1 read of lane 31)
 constexpr int kRing = 4;     // staged node rows in flight / in use per warp
@@ -139,9 +141,6 @@ struct MechKT {
   const T* invM;
   const T* rf;
   const T* gpm;  // finest level, precomputed Gauss-point moduli: K - 2G/3 at [g * n + e], G at [(8 + g) * n + e]
-  T* zout;       // RESIDUAL: z = M^-1 r written here when not null
-  T* pnew;       // PCGDIR: the new direction, written by each node's owner
-  int s_bnum, s_bden, first;  // PCGDIR: beta = scal[s_bnum] / scal[s_bden], 0 when first
   RedTarget red;
   double* err;   // tensor-core kernel: set to 1 when a bounded wait ran out
 };
@@ -233,20 +232,14 @@ __device__ __forceinline__ void assemble_row(const MechKT<T>& k, const Stream<NF
           if (k.red.slot[0] >= 0) red0 = fma((double)fv, (double)fv, red0);  // sums nobody reads are skipped
           const T rv = fix[m] ? T(0) : fv - tot[m];
           k.out[n + m * N] = rv;
-          if (k.invM) {
-            const T zv = rv * k.invM[n + m * N];
-            if (k.zout) k.zout[n + m * N] = zv;
-            red1 = fma((double)rv, (double)zv, red1);
-          }
+          if (k.invM) red1 = fma((double)rv, (double)(rv * k.invM[n + m * N]), red1);
           if (k.red.slot[2] >= 0) red2 = fma((double)rv, (double)rv, red2);
         }
-      } else if (EPI == EPI_PCG || EPI == EPI_PCGDIR) {  // w = K p, (p, w); PCGDIR: the owner writes p
+      } else if (EPI == EPI_PCG) {  // w = K p, (p, w)
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-          const T pv = st.at(si - 1, m, 0, lane);
           k.out[n + m * N] = tot[m];
-          if (EPI == EPI_PCGDIR) k.pnew[n + m * N] = pv;
-          red0 = fma((double)pv, (double)tot[m], red0);
+          red0 = fma((double)st.at(si - 1, m, 0, lane), (double)tot[m], red0);
         }
       } else if (EPI == EPI_FAS) {
         // coarsen_f_standard_routine (multigrid_intergrid.cpp:124-342) fused with the coarse apply
@@ -271,25 +264,18 @@ __device__ __forceinline__ void assemble_row(const MechKT<T>& k, const Stream<NF
 // T = double: the plain form; T = float: the precision form's V-cycle (reductions stay FP64).
 // GPM: the finest level's Gauss-point moduli come precomputed (gp_material_kernel) instead of being
 // interpolated from the staged nodal K, G, d in every apply.
-// EPI_PCGDIR (FINEST && GPM): the staged fields are z = M^-1 r (0..2) and the previous direction
-// (3..5); each lane turns its column of a row that has landed into p = z + beta p_old in place, before
-// any lane reads the row, so the element math sees p.  (A call's first iteration passes z as p_old
-// with beta = 0: fma(0, z, z) = z.)
 template <typename T, bool FINEST, int EPI, bool DIAG, bool ISO, bool GPM = false>
 __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
   constexpr int NU = DIAG ? 0 : 3;
-  constexpr bool PDIR = EPI == EPI_PCGDIR;
-  static_assert(!PDIR || (FINEST && GPM && !DIAG), "the fused direction update runs on precomputed moduli");
-  constexpr int NF = PDIR ? 6 : NU + (FINEST ? (GPM ? 0 : 3) : 2);
+  constexpr int NF = NU + (FINEST ? (GPM ? 0 : 3) : 2);
   extern __shared__ __align__(16) unsigned char mech_smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  T* ring = reinterpret_cast<T*>(mech_smem) + (size_t)wib * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32);
+  // per warp: the staging ring, then the z-carry of the strip's wy - 1 output rows
+  T* ring = reinterpret_cast<T*>(mech_smem) + (size_t)wib * (kRing * NF * 2 * kRowW + (k.sg.wy - 1) * 3 * 32);
   T* zc = ring + kRing * NF * 2 * kRowW;  // [row][comp][lane]
   const SFt<T> s = make_sf<T>(k.g);
   double red0 = 0.0, red1 = 0.0, red2 = 0.0;
   const long long nwarps_total = (long long)gridDim.x * kWarps;
-  T beta = T(0);
-  if (PDIR && !k.first) beta = (T)(k.red.scal[k.s_bnum] / k.red.scal[k.s_bden]);
   const T* fptr[NF];
 #pragma unroll
   for (int f = 0; f < NF; ++f) fptr[f] = k.fields[f];
@@ -312,17 +298,6 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
       st.issue(si + 2, lane);
       cp_async_wait2();
       __syncwarp();
-      if constexpr (PDIR) {  // p = z + beta p_old on this lane's column of the row that just landed
-        T* slot = ring + (size_t)(si & (kRing - 1)) * NF * 2 * kRowW;
-#pragma unroll
-        for (int m = 0; m < 3; ++m)
-#pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            T* zp = slot + (m * 2 + c) * kRowW + lane;
-            *zp = fma(beta, slot[((3 + m) * 2 + c) * kRowW + lane], *zp);
-          }
-        __syncwarp();
-      }
       const int li = si / rows, r = si - li * rows;
       const int kk = z0 - 1 + li;
       if (r == 0) {
@@ -402,7 +377,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
       __syncwarp();
     }
   }
-  if (EPI == EPI_RESIDUAL || EPI == EPI_PCG || EPI == EPI_PCGDIR) {
+  if (EPI == EPI_RESIDUAL || EPI == EPI_PCG) {
     double v[3] = {red0, red1, red2};
     grid_reduce<3>(v, k.red);
   }
@@ -533,7 +508,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_tc_kernel(MechKT<float> k) {
   uint64_t* bar = reinterpret_cast<uint64_t*>(tc_smem + kTcABytes + kTcB1Bytes + kTcB2Bytes);
   uint32_t* taddr_s = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
-  T* ring = reinterpret_cast<T*>(tc_smem + kTcHead) + (size_t)wib * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32);
+  T* ring = reinterpret_cast<T*>(tc_smem + kTcHead) + (size_t)wib * (kRing * NF * 2 * kRowW + (k.sg.wy - 1) * 3 * 32);
   T* zc = ring + kRing * NF * 2 * kRowW;
   const SFt<T> s = make_sf<T>(k.g);
   const uint32_t sA = (uint32_t)__cvta_generic_to_shared(As), sB1 = (uint32_t)__cvta_generic_to_shared(B1s);
@@ -762,33 +737,44 @@ RedTarget make_red(hpc_ctx* c, int s0, int s1, int s2) {
 // Per-kernel launch configuration (dynamic shared-memory opt-in and resident blocks per SM), set up
 // on a kernel's first launch so that later launches - also those inside a stream capture - only
 // enqueue work.
+// Dynamic shared memory of a strip kernel as a function of the strip height wy: `fixed` bytes, then
+// per warp a staging ring of `ring` elements and a z-carry of `row` elements per output row
+// (wy - 1 rows), elements of `elem` bytes.
+struct SmemPlan {
+  size_t fixed, ring, row, elem;
+  size_t bytes(int wy) const { return fixed + (size_t)kWarps * (ring + (size_t)(wy - 1) * row) * elem; }
+};
+
+// Per kernel and dynamic shared-memory size: the opt-in and resident blocks per SM, set up on first
+// use so that later launches - also those inside a stream capture - only enqueue work.
 struct KernelCfg {
   const void* fn;
   int device;
+  size_t smem;
   int per_sm;
 };
 static std::mutex g_cfg_mu;
-static KernelCfg g_cfg[128];
+static KernelCfg g_cfg[512];
 static int g_ncfg = 0;
 
 template <class Kern>
-static int kernel_cfg(Kern kern, size_t smem, int* per_sm_out) {
+static int kernel_cfg(Kern kern, size_t max_smem, size_t smem, int* per_sm_out) {
   int dev = 0;
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lock(g_cfg_mu);
   for (int i = 0; i < g_ncfg; ++i)
-    if (g_cfg[i].fn == (const void*)kern && g_cfg[i].device == dev) {
+    if (g_cfg[i].fn == (const void*)kern && g_cfg[i].device == dev && g_cfg[i].smem == smem) {
       *per_sm_out = g_cfg[i].per_sm;
       return HPC_OK;
     }
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (max_smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(smem)");
   }
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWarps * 32, smem);
   if (e != cudaSuccess || per_sm <= 0) per_sm = 1;
-  if (g_ncfg < 128) g_cfg[g_ncfg++] = KernelCfg{(const void*)kern, dev, per_sm};
+  if (g_ncfg < 512) g_cfg[g_ncfg++] = KernelCfg{(const void*)kern, dev, smem, per_sm};
   *per_sm_out = per_sm;
   return HPC_OK;
 }
@@ -823,7 +809,7 @@ static int grid_for(const StripGeo& sg, long long cap) {
 // Times every candidate shape on the live arguments (element kernels are pure functions of their
 // inputs: a repeated launch rewrites the same outputs and reductions) and keeps the fastest.
 template <class Kern, class Args>
-static int autotune_shape(hpc_ctx* c, Kern kern, Args a, size_t smem, long long cap, StripGeo* best, int ox) {
+static int autotune_shape(hpc_ctx* c, Kern kern, Args a, const SmemPlan& plan, StripGeo* best, int ox) {
   static const int wys[] = {8, 4, 2};
   static const int czs[] = {32, 16, 8, 4, 2};
   cudaEvent_t e0, e1;
@@ -832,10 +818,13 @@ static int autotune_shape(hpc_ctx* c, Kern kern, Args a, size_t smem, long long 
   float best_ms = 1e30f;
   *best = choose_strips(a.g, (long long)num_sms() * 4, ox);
   int rc = HPC_OK;
-  for (int wy : wys)
+  for (int wy : wys) {
     for (int cz : czs) {
       a.sg = strip_geo(a.g, wy, cz, ox);
-      const int grid = grid_for(a.sg, cap);
+      const size_t smem = plan.bytes(wy);
+      int per_sm = 1;
+      if ((rc = kernel_cfg(kern, plan.bytes(kWY), smem, &per_sm))) break;
+      const int grid = grid_for(a.sg, (long long)num_sms() * per_sm);
       if (grid <= 0 || (size_t)grid * 3 > c->partials_cap) continue;
       kern<<<grid, kWarps * 32, smem, c->stream>>>(a);
       cudaEventRecord(e0, c->stream);
@@ -856,6 +845,8 @@ static int autotune_shape(hpc_ctx* c, Kern kern, Args a, size_t smem, long long 
         *best = a.sg;
       }
     }
+    if (rc) break;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
@@ -867,18 +858,16 @@ static int autotune_shape(hpc_ctx* c, Kern kern, Args a, size_t smem, long long 
 // measured it before.
 // `units`: the strip-shape model's parallel units (0: the SM sub-partitions).
 template <class Kern, class Args>
-static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls, int ox = kOX, long long units = 0) {
-  int per_sm = 1;
-  int rc = kernel_cfg(kern, smem, &per_sm);
-  if (rc) return rc;
-  const long long cap = (long long)num_sms() * per_sm;
+static int launch_strips(hpc_ctx* c, Kern kern, Args a, const SmemPlan& plan, int cls, int ox = kOX,
+                         long long units = 0) {
+  int rc = HPC_OK;
   if (units <= 0) units = (long long)num_sms() * 4;
   int dev = 0;
   cudaGetDevice(&dev);
   if (!tuned_shape((const void*)kern, dev, a.g, &a.sg, ox)) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (c->autotune && cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
-      if ((rc = autotune_shape(c, kern, a, smem, cap, &a.sg, ox))) return rc;
+      if ((rc = autotune_shape(c, kern, a, plan, &a.sg, ox))) return rc;
       std::lock_guard<std::mutex> lock(g_tune_mu);
       if (g_ntuned < 512)
         g_tuned[g_ntuned++] = TunedShape{(const void*)kern, dev, a.g.nx, a.g.ny, a.g.nz, a.sg.wy, a.sg.cz};
@@ -886,7 +875,10 @@ static int launch_strips(hpc_ctx* c, Kern kern, Args a, size_t smem, int cls, in
       a.sg = choose_strips(a.g, units, ox);
     }
   }
-  const int grid = grid_for(a.sg, cap);
+  const size_t smem = plan.bytes(a.sg.wy);
+  int per_sm = 1;
+  if ((rc = kernel_cfg(kern, plan.bytes(kWY), smem, &per_sm))) return rc;
+  const int grid = grid_for(a.sg, (long long)num_sms() * per_sm);
   if (grid <= 0) return HPC_OK;
   if ((size_t)grid * 3 > c->partials_cap) return cuda_fail(cudaErrorInvalidValue, "partials buffer");
   timing_begin(c, cls);
@@ -915,37 +907,22 @@ inline bool iso(const LevelGeo& g) { return g.hx == g.hy && g.hy == g.hz; }
 
 template <bool F, int E, bool D, typename T = double>
 static int run_mech(hpc_ctx* c, const MechKT<T>& k) {
-  const int cls = (F && (E == EPI_PCG || E == EPI_PCGDIR) && !D)
-                      ? (sizeof(T) == 8 ? HPC_KC_MECH_PCG_FINEST : HPC_KC_MECH32_PCG_FINEST)
-                      : HPC_KC_NONE;
-  if constexpr (E == EPI_PCGDIR) {
-    static_assert(F && !D, "fused direction update: finest PCG apply only");
-    if (!k.gpm) {
-      set_error("fused direction update without precomputed Gauss-point moduli");
-      return HPC_ERR_ARG;
-    }
-    constexpr int NF = 6;  // z and the previous direction
-    const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
-    if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true, true>, k, smem, cls);
-    return launch_strips(c, mech_kernel<T, F, E, D, false, true>, k, smem, cls);
-  }
-  if constexpr (F && !D && E != EPI_PCGDIR) {
+  const int cls = (F && E == EPI_PCG && !D) ? (sizeof(T) == 8 ? HPC_KC_MECH_PCG_FINEST : HPC_KC_MECH32_PCG_FINEST)
+                                             : HPC_KC_NONE;
+  if constexpr (F && !D) {
     if (k.gpm) {  // precomputed Gauss-point moduli: only u is staged
       constexpr int NF = 3;
-      const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
+      const SmemPlan smem{0, (size_t)kRing * NF * 2 * kRowW, 3 * 32, sizeof(T)};
       if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true, true>, k, smem, cls);
       return launch_strips(c, mech_kernel<T, F, E, D, false, true>, k, smem, cls);
     }
   }
-  if constexpr (E != EPI_PCGDIR) {
-    constexpr int NF = (D ? 0 : 3) + (F ? 3 : 2);
-    const size_t smem = (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(T);
-    if constexpr (!D) {
-      if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true>, k, smem, cls);
-    }
-    return launch_strips(c, mech_kernel<T, F, E, D, false>, k, smem, cls);
+  constexpr int NF = (D ? 0 : 3) + (F ? 3 : 2);
+  const SmemPlan smem{0, (size_t)kRing * NF * 2 * kRowW, 3 * 32, sizeof(T)};
+  if constexpr (!D) {
+    if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true>, k, smem, cls);
   }
-  return HPC_ERR_ARG;
+  return launch_strips(c, mech_kernel<T, F, E, D, false>, k, smem, cls);
 }
 
 static void mech_fields(hpc_ctx* c, int level, bool finest, bool diag, const double* src, MechK& k) {
@@ -979,23 +956,8 @@ int launch_mech(hpc_ctx* c, const MechCall& m) {
   k.rf = m.rf;
   k.gpm = (m.finest && c->gpm_active) ? c->F[m.level].gpm : nullptr;
   k.red = make_red(c, m.s_out0, m.s_out1, m.s_out2);
-  k.zout = m.zout;
-  if (m.epi == EPI_PCGDIR) {
-    const long long n = c->L[m.level].n;
-    for (int q = 0; q < 3; ++q) k.fields[3 + q] = (m.first ? m.src : m.pold) + (long long)q * n;
-    k.pnew = m.pnew;
-    k.s_bnum = m.s_bnum;
-    k.s_bden = m.s_bden;
-    k.first = m.first ? 1 : 0;
-  }
   const bool f = m.finest;
   switch (m.epi) {
-    case EPI_PCGDIR:
-      if (!f) {
-        set_error("fused direction update on a coarse level");
-        return HPC_ERR_ARG;
-      }
-      return run_mech<true, EPI_PCGDIR, false>(c, k);
     case EPI_PLAIN: return f ? run_mech<true, EPI_PLAIN, false>(c, k) : run_mech<false, EPI_PLAIN, false>(c, k);
     case EPI_RESIDUAL:
       return f ? run_mech<true, EPI_RESIDUAL, false>(c, k) : run_mech<false, EPI_RESIDUAL, false>(c, k);
@@ -1021,7 +983,7 @@ int launch_mech_diag(hpc_ctx* c, int level, bool finest, double small_k, double*
 template <bool F, int E>
 static int run_mech_tc(hpc_ctx* c, const MechKT<float>& k) {
   constexpr int NF = 3 + (F ? 0 : 2);
-  const size_t smem = (size_t)kTcHead + (size_t)kWarps * (kRing * NF * 2 * kRowW + (kWY - 1) * 3 * 32) * sizeof(float);
+  const SmemPlan smem{(size_t)kTcHead, (size_t)kRing * NF * 2 * kRowW, 3 * 32, sizeof(float)};
   // strip shapes of the latency model (one lockstep block per SM on the large levels); shapes that
   // give every resident block (3 per SM) strips measured slower (MMA round trips share the SM)
   return launch_strips(c, mech_tc_kernel<F, E>, k, smem, (F && E == EPI_PCG) ? HPC_KC_MECH32_PCG_FINEST : HPC_KC_NONE);
@@ -1139,7 +1101,7 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
   constexpr int NF = 3;
   extern __shared__ double smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  double* ring = smem + (size_t)wib * (kRing * NF * 2 * kRowW + (kWY - 1) * 32);
+  double* ring = smem + (size_t)wib * (kRing * NF * 2 * kRowW + (k.sg.wy - 1) * 32);
   double* zc = ring + kRing * NF * 2 * kRowW;  // [row][lane]
   const SF s = make_sf(k.g);
   double red0 = 0.0, red1 = 0.0, red2 = 0.0;
@@ -1250,7 +1212,7 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
 
 template <int E, bool D>
 static int run_pf(hpc_ctx* c, const PfK& k, bool finest) {
-  const size_t smem = (size_t)kWarps * (kRing * 3 * 2 * kRowW + (kWY - 1) * 32) * sizeof(double);
+  const SmemPlan smem{0, (size_t)kRing * 3 * 2 * kRowW, 32, sizeof(double)};
   const int cls = (finest && E == EPI_PCG && !D) ? HPC_KC_PF_PCG_FINEST : HPC_KC_NONE;
   if constexpr (!D) {
     if (iso(k.g)) return launch_strips(c, pf_kernel<E, D, true>, k, smem, cls);

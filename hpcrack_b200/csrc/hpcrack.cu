@@ -7,6 +7,7 @@
 // the reference tests it) and at the end of a call.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -104,7 +105,7 @@ static bool geometry_ok(const hpc_geometry* g) {
 // Number of doubles per level allocated for a level with n padded slots.
 constexpr int kScalarFieldsPerLevel = 10;  // bulK G gc d H fd Ke Ge R dold
 constexpr int kVectorFieldsPerLevel = 4;   // u fu ru uold
-constexpr int kWork3 = 4, kWork1 = 4;      // preMu p w z / preMd pd wd tmp1
+constexpr int kWork3 = 4, kWork1 = 4;      // preMu p w tmp3 / preMd pd wd tmp1
 static size_t level_bytes(long long n) {
   return (size_t)n * sizeof(double) * (kScalarFieldsPerLevel + 3 * kVectorFieldsPerLevel + 3 * kWork3 + kWork1) +
          (size_t)n;  // choice
@@ -183,7 +184,7 @@ static void shape_table(double N[64]) {
 static bool is_finest(hpc_ctx* c, int l) { return l == c->maxlevel; }
 
 // Every level's zero-diagonal count goes to its own slot; one read checks them all.
-static int check_zero_diags(hpc_ctx* c, int top, const char* what) {
+int check_zero_diags(hpc_ctx* c, int top, const char* what) {
   double z[kMaxLevels];
   int rc = read_scalars(c, S_ZEROS, top + 1, z);
   if (rc) return rc;
@@ -196,7 +197,7 @@ static int check_zero_diags(hpc_ctx* c, int top, const char* what) {
 }
 
 // diag K(d) of every level 0..top into preMu; fails like the reference on a zero entry.
-static int mech_diags(hpc_ctx* c, int top, double small_k) {
+int mech_diags(hpc_ctx* c, int top, double small_k) {
   for (int l = 0; l <= top; ++l) {
     int rc = launch_mech_diag(c, l, is_finest(c, l), small_k, c->F[l].preMu);
     if (rc) return rc;
@@ -205,7 +206,7 @@ static int mech_diags(hpc_ctx* c, int top, double small_k) {
   }
   return check_zero_diags(c, top, "PreM_u");
 }
-static int pf_diags(hpc_ctx* c, int top, double lc) {
+int pf_diags(hpc_ctx* c, int top, double lc) {
   for (int l = 0; l <= top; ++l) {
     int rc = launch_pf_diag(c, l, lc, c->F[l].preMd);
     if (rc) return rc;
@@ -235,39 +236,7 @@ static int pcg_u_dev(hpc_ctx* c, int l, double small_k, double Ut, int nb, int t
   m.s_out0 = m.set_fnorm ? S_FNORM : -1;
   m.s_out1 = slot_rz(0);
   m.s_out2 = S_RNORM;
-  // Finest level with the precomputed Gauss-point moduli: the direction update p = M^-1 r + beta p
-  // happens inside the apply's staging (EPI_PCGDIR) from z = M^-1 r, which the residual and the
-  // updates write; the directions alternate between two buffers, since neighbouring strips still read
-  // the old direction while a node's owner writes the new one.  Same products and fma as the
-  // separate pass, so the same bits.
-  const bool fuse = m.finest && c->fused_dir && c->gpm_active && F.p2 && nb > 0;
-  if (fuse) m.zout = F.z;
   if ((rc = launch_mech(c, m))) return rc;
-  if (fuse) {
-    double* dirs[2] = {F.p, F.p2};
-    for (int it = 0; it < nb; ++it) {
-      MechCall q{};
-      q.level = l;
-      q.finest = true;
-      q.epi = EPI_PCGDIR;
-      q.src = F.z;
-      q.pold = dirs[it & 1];
-      q.pnew = dirs[(it + 1) & 1];
-      q.first = it == 0;
-      q.s_bnum = slot_rz(it);
-      q.s_bden = slot_rz(it - 1);
-      q.out = F.w;
-      q.small_k = small_k;
-      q.s_out0 = slot_pw(it);
-      q.s_out1 = q.s_out2 = -1;
-      if ((rc = launch_mech(c, q))) return rc;
-      // z for the next iteration's apply (none after the last: the next call starts from a residual)
-      if ((rc = launch_mech_update_on(c, l, F.u, F.ru, q.pnew, F.w, F.preMu, slot_rz(it), slot_pw(it),
-                                      slot_rz(it + 1), slot_rn(it), it + 1 < nb ? F.z : nullptr)))
-        return rc;
-    }
-    return HPC_OK;
-  }
   for (int it = 0; it < nb; ++it) {
     if ((rc = launch_dir_update(c, l, 3, F.ru, F.preMu, F.p, it == 0, slot_rz(it), slot_rz(it - 1)))) return rc;
     MechCall q{};
@@ -401,9 +370,7 @@ static bool same_mg(const hpc_mg& a, const hpc_mg& b) {
 // parameters differ from the cached ones (the kernels' first use must already have happened,
 // `allow_capture`), replayed afterwards.  Kernel launches are counted per replay.  A graph is keyed
 // by its parameters and by `flags`, the context's kernel choices baked into its launches.
-static int graph_flags(const hpc_ctx* c) {
-  return c->fused_dir * 8 + c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active;
-}
+static int graph_flags(const hpc_ctx* c) { return c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active; }
 template <class Body>
 static int run_graphed(hpc_ctx* c, hpc_ctx::CoarseGraph& g, const hpc_mg& mg, double a, double b, bool allow_capture,
                        Body body, int flags) {
@@ -442,7 +409,7 @@ static int run_graphed(hpc_ctx* c, hpc_ctx::CoarseGraph& g, const hpc_mg& mg, do
 
 // Top-level cycles of the solves: the finest level's smoothing is launched directly (its kernels
 // are large and individually timed), everything below it is replayed as one graph.
-static int cycle_u_top(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, bool allow_capture) {
+int cycle_u_top(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, bool allow_capture) {
   const int L = c->maxlevel;
   long long it = 0;
   if (L == 0) return cycle_u_dev(c, 0, mg, small_k, Ut, t, &it);
@@ -454,7 +421,7 @@ static int cycle_u_top(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, 
   return pcg_u_dev(c, L, small_k, Ut, mg.nu2, t);
 }
 
-static int cycle_d_top(hpc_ctx* c, const hpc_mg& mg, double lc, bool allow_capture) {
+int cycle_d_top(hpc_ctx* c, const hpc_mg& mg, double lc, bool allow_capture) {
   const int L = c->maxlevel;
   long long it = 0;
   if (L == 0) return cycle_d_dev(c, 0, mg, lc, &it);
@@ -470,7 +437,7 @@ static int cycle_d_top(hpc_ctx* c, const hpc_mg& mg, double lc, bool allow_captu
 
 // Per-level element moduli for the mechanical solve: MP_choice + MP_all_element on the finest level,
 // then VR_all_level for K_element and G_element (mechanical_displacement.cpp:33-45).
-static int mech_material(hpc_ctx* c, double small_k) {
+int mech_material(hpc_ctx* c, double small_k) {
   int rc;
   const int L = c->maxlevel;
   if ((rc = launch_choice_level(c, L, small_k, true, true))) return rc;
@@ -488,17 +455,12 @@ struct GpmScope {
   explicit GpmScope(hpc_ctx* ctx) : c(ctx) {}
   ~GpmScope() { c->gpm_active = 0; }
 };
-static int gp_material(hpc_ctx* c, double small_k) {
+int gp_material(hpc_ctx* c, double small_k) {
   LevelFields& F = c->F[c->maxlevel];
   if (!F.gpm) {
     const size_t bytes = sizeof(double) * 16 * (size_t)c->L[c->maxlevel].n;
     HPC_CUDA(cudaMalloc((void**)&F.gpm, bytes));
     HPC_CUDA(cudaMemsetAsync(F.gpm, 0, bytes, c->stream));  // non-element slots stay zero
-  }
-  if (!F.p2) {  // the second direction buffer of the fused direction update (same first use)
-    const size_t bytes = sizeof(double) * 3 * (size_t)c->L[c->maxlevel].n;
-    HPC_CUDA(cudaMalloc((void**)&F.p2, bytes));
-    HPC_CUDA(cudaMemsetAsync(F.p2, 0, bytes, c->stream));  // padding slots stay zero
   }
   int rc = launch_gp_material(c, small_k);
   if (rc) return rc;
@@ -569,7 +531,7 @@ static int u_entire_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut,
 // The preconditioner of the mixed-precision solve: one V-cycle of cycle_u's kind (restarted
 // Jacobi-PCG smoothing, injection, FAS right-hand side, prolongation) on single-precision copies of
 // the levels, solving for a correction (homogeneous Dirichlet values).  Its coarsest solve stays FP64.
-static int ensure_f32(hpc_ctx* c) {
+int ensure_f32(hpc_ctx* c) {
   if (c->F32[0].u) return HPC_OK;
   for (int l = 0; l <= c->maxlevel; ++l) {
     const size_t n = (size_t)c->L[l].n;
@@ -596,7 +558,7 @@ static int ensure_f32(hpc_ctx* c) {
 }
 
 // FP32 material and inverse diagonals from the FP64 ones (after mech_material and mech_diags).
-static int f32_material(hpc_ctx* c) {
+int f32_material(hpc_ctx* c) {
   int rc;
   for (int l = 0; l <= c->maxlevel; ++l) {
     const long long n = c->L[l].n;
@@ -698,7 +660,7 @@ static int cycle_u32(hpc_ctx* c, int l, const hpc_mg& mg, double small_k) {
 }
 
 // ---------------------------------------------------------------- flexible PCG (precision form)
-static int ensure_fcg(hpc_ctx* c) {
+int ensure_fcg(hpc_ctx* c) {
   if (c->fcg.x) return HPC_OK;
   const size_t bytes = sizeof(double) * 3 * (size_t)c->L[c->maxlevel].n;
   double** arrs[] = {&c->fcg.x, &c->fcg.r, &c->fcg.rp, &c->fcg.f, &c->fcg.p};
@@ -711,7 +673,7 @@ static int ensure_fcg(hpc_ctx* c) {
 
 // True residual r = f - K x with Dirichlet rows zero; at t == 0 the reactions of x become f's
 // Dirichlet rows and f_norm (as every finest pcg_u call at t == 0 does, mechanical_pcg.cpp:252-258).
-static int fcg_residual(hpc_ctx* c, double small_k, int t, int s_rn) {
+int fcg_residual(hpc_ctx* c, double small_k, int t, int s_rn) {
   const int L = c->maxlevel;
   MechCall m{};
   m.level = L;
@@ -727,6 +689,70 @@ static int fcg_residual(hpc_ctx* c, double small_k, int t, int s_rn) {
   m.s_out1 = -1;
   m.s_out2 = s_rn;
   return launch_mech(c, m);
+}
+
+// One flexible-PCG iteration k of the mechanical solve (the part without a host read): the
+// preconditioning V-cycle (FP32 mirror when mixed), delta / gamma, the direction, w = K p and the
+// x / r update.  coarse_graph: replay the cycle's coarse part from its cached graph.
+int fcg_iteration(hpc_ctx* c, const hpc_mg& mg, double small_k, int k, bool mixed, bool coarse_graph) {
+  const int L = c->maxlevel;
+  LevelFields& F = c->F[L];
+  const LevelGeo& g = c->L[L];
+  const size_t vbytes = sizeof(double) * 3 * (size_t)g.n;
+  int r2;
+  // z = V-cycle on A z = r from z = 0 with homogeneous Dirichlet values: u is the cycle's unknown,
+  // fu its right-hand side
+  if (mixed) {  // the same cycle on the FP32 mirror; z comes back to F.u in FP64
+    const LevelF32& G = c->F32[L];
+    HPC_CUDA(cudaMemsetAsync(G.u, 0, 3 * (size_t)g.n * sizeof(float), c->stream));
+    if ((r2 = launch_to_f32(c, c->fcg.r, G.fu, 3 * g.n))) return r2;
+    if (L == 0) {
+      if ((r2 = cycle_u32(c, 0, mg, small_k))) return r2;
+    } else {
+      if ((r2 = pcg_u32(c, L, small_k, mg.nu1, true))) return r2;
+      if (coarse_graph) {
+        if ((r2 = run_graphed(c, c->g32, mg, small_k, 0.0, k > 0, [&] { return coarse_part_u32(c, L, mg, small_k); },
+                              graph_flags(c))))
+          return r2;
+      } else if ((r2 = coarse_part_u32(c, L, mg, small_k))) {
+        return r2;
+      }
+      if ((r2 = pcg_u32(c, L, small_k, mg.nu2))) return r2;
+    }
+  } else {
+    HPC_CUDA(cudaMemsetAsync(F.u, 0, vbytes, c->stream));
+    HPC_CUDA(cudaMemcpyAsync(F.fu, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+    if ((r2 = cycle_u_top(c, mg, small_k, 0.0, 1, k > 0))) return r2;
+  }
+  // delta_k = (z, r_k), gamma_k = (z, r_{k-1}); p = z + beta p.  The precision form reads z from the
+  // FP32 cycle directly (its FP64 copy would be exact).
+  if (mixed) {
+    const float* z = c->F32[L].u;
+    if ((r2 = launch_dot2(c, L, z, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k))))
+      return r2;
+    if ((r2 = launch_fcg_dir(c, L, z, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
+      return r2;
+  } else {
+    if ((r2 = launch_dot2(c, L, F.u, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k))))
+      return r2;
+    if ((r2 = launch_fcg_dir(c, L, F.u, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
+      return r2;
+  }
+  // w = K p, (p, w); the smoothers' own p and w are free between V-cycles
+  MechCall q{};
+  q.level = L;
+  q.finest = true;
+  q.epi = EPI_PCG;
+  q.src = c->fcg.p;
+  q.out = F.w;
+  q.small_k = small_k;
+  q.s_out0 = slot_fpw(k);
+  q.s_out1 = q.s_out2 = -1;
+  if ((r2 = launch_mech(c, q))) return r2;
+  // r_{k-1} kept for the flexible beta; x += alpha p, r -= alpha w, alpha = delta_k / (p, w)
+  HPC_CUDA(cudaMemcpyAsync(c->fcg.rp, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
+  return launch_mech_update_on(c, L, c->fcg.x, c->fcg.r, c->fcg.p, F.w, F.preMu, slot_fdelta(k), slot_fpw(k),
+                               slot_fdummy(k), slot_frn(k));
 }
 
 // The mechanical solve of u_entire (mechanical_displacement.cpp:25-115) by flexible PCG on the finest
@@ -770,62 +796,7 @@ static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double
   const bool whole_graph = mixed && c->use_graphs && c->timing_class < 0;
   for (int k = 0; k < mg.ncy; ++k) {
     if (rel <= mech_tol && !(t == 0 && k == 0)) break;  // one iteration forced at t == 0 (:74, :84-85)
-    auto iteration = [&](bool coarse_graph) -> int {
-      int r2;
-      // z = V-cycle on A z = r from z = 0 with homogeneous Dirichlet values: u is the cycle's unknown,
-      // fu its right-hand side
-      if (mixed) {  // the same cycle on the FP32 mirror; z comes back to F.u in FP64
-        const LevelF32& G = c->F32[L];
-        HPC_CUDA(cudaMemsetAsync(G.u, 0, 3 * (size_t)g.n * sizeof(float), c->stream));
-        if ((r2 = launch_to_f32(c, c->fcg.r, G.fu, 3 * g.n))) return r2;
-        if (L == 0) {
-          if ((r2 = cycle_u32(c, 0, mg, small_k))) return r2;
-        } else {
-          if ((r2 = pcg_u32(c, L, small_k, mg.nu1, true))) return r2;
-          if (coarse_graph) {
-            if ((r2 = run_graphed(c, c->g32, mg, small_k, 0.0, k > 0, [&] { return coarse_part_u32(c, L, mg, small_k); },
-                                  graph_flags(c))))
-              return r2;
-          } else if ((r2 = coarse_part_u32(c, L, mg, small_k))) {
-            return r2;
-          }
-          if ((r2 = pcg_u32(c, L, small_k, mg.nu2))) return r2;
-        }
-      } else {
-        HPC_CUDA(cudaMemsetAsync(F.u, 0, vbytes, c->stream));
-        HPC_CUDA(cudaMemcpyAsync(F.fu, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
-        if ((r2 = cycle_u_top(c, mg, small_k, 0.0, 1, k > 0))) return r2;
-      }
-      // delta_k = (z, r_k), gamma_k = (z, r_{k-1}); p = z + beta p.  The precision form reads z from the
-      // FP32 cycle directly (its FP64 copy would be exact).
-      if (mixed) {
-        const float* z = c->F32[L].u;
-        if ((r2 = launch_dot2(c, L, z, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k))))
-          return r2;
-        if ((r2 = launch_fcg_dir(c, L, z, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
-          return r2;
-      } else {
-        if ((r2 = launch_dot2(c, L, F.u, c->fcg.r, k > 0 ? c->fcg.rp : nullptr, slot_fdelta(k), slot_fgamma(k))))
-          return r2;
-        if ((r2 = launch_fcg_dir(c, L, F.u, c->fcg.p, k == 0, slot_fdelta(k), slot_fgamma(k), slot_fdelta(k - 1))))
-          return r2;
-      }
-      // w = K p, (p, w); the smoothers' own p and w are free between V-cycles
-      MechCall q{};
-      q.level = L;
-      q.finest = true;
-      q.epi = EPI_PCG;
-      q.src = c->fcg.p;
-      q.out = F.w;
-      q.small_k = small_k;
-      q.s_out0 = slot_fpw(k);
-      q.s_out1 = q.s_out2 = -1;
-      if ((r2 = launch_mech(c, q))) return r2;
-      // r_{k-1} kept for the flexible beta; x += alpha p, r -= alpha w, alpha = delta_k / (p, w)
-      HPC_CUDA(cudaMemcpyAsync(c->fcg.rp, c->fcg.r, vbytes, cudaMemcpyDeviceToDevice, c->stream));
-      return launch_mech_update_on(c, L, c->fcg.x, c->fcg.r, c->fcg.p, F.w, F.preMu, slot_fdelta(k), slot_fpw(k),
-                                   slot_fdummy(k), slot_frn(k));
-    };
+    auto iteration = [&](bool coarse_graph) -> int { return fcg_iteration(c, mg, small_k, k, mixed, coarse_graph); };
     if (whole_graph) {
       // graph key: the cycle parameters, small_k and the kernel choices baked into the launches
       hpc_ctx::CoarseGraph& gk = c->gfcg[k == 0 ? 0 : ((k & 1) ? 1 : 2)];
@@ -922,7 +893,7 @@ static int phase_field_dev(hpc_ctx* c, const hpc_mg& mg, double lc, double pf_to
   return HPC_OK;
 }
 
-static int voigt_all_level(hpc_ctx* c, int field) {
+int voigt_all_level(hpc_ctx* c, int field) {
   int rc;
   for (int l = c->maxlevel; l > 0; --l)
     if ((rc = launch_vr(c, l, scalar_field(c, field, l), scalar_field(c, field, l - 1), false, false))) return rc;
@@ -954,10 +925,9 @@ int hpc_footprint(const hpc_geometry* geo, size_t* bytes) {
   const size_t nf = (size_t)f.px * f.ny * f.nz;
   total += nf * sizeof(double);  // d_old
   total += sizeof(double) * (kScalarPool + 3 * 8192) + 64;
-  // allocated on first use: Gauss-point moduli (16 n) with the second PCG direction (3n),
-  // flexible-PCG vectors (5 x 3n), the FP32 mirror of every level (7 x 3n + material) with its
-  // Gauss-point moduli, the checkpoint (6 dense)
-  total += nf * sizeof(double) * (16 + 3 + 15);
+  // allocated on first use: Gauss-point moduli (16 n), flexible-PCG vectors (5 x 3n), the FP32
+  // mirror of every level (7 x 3n + material) with its Gauss-point moduli, the checkpoint (6 dense)
+  total += nf * sizeof(double) * (16 + 15);
   for (int l = 0; l <= geo->maxlevel; ++l) {
     const size_t n = (size_t)lv[l].px * lv[l].ny * lv[l].nz;
     total += n * sizeof(float) * (21 + (l == geo->maxlevel ? 3 + 16 : 2));
@@ -967,6 +937,8 @@ int hpc_footprint(const hpc_geometry* geo, size_t* bytes) {
   *bytes = total;
   return HPC_OK;
 }
+
+static std::atomic<unsigned long long> g_ctx_uid{0};
 
 int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   if (!out) return arg_fail("null output");
@@ -987,8 +959,8 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   c->device = device;
   c->choice_quirk = 1;
   c->use_graphs = 1;
+  c->uid = ++g_ctx_uid;
   c->fused_coarsest = 1;
-  c->fused_dir = 0;  // measured slower than the separate pass on B200 (hpc_set_fused_direction)
   c->timing_class = HPC_KC_NONE;
   HostLevel lv[kMaxLevels];
   host_geometry(*geo, c->box, lv);
@@ -1048,7 +1020,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
     const long long n = c->L[l].n;
     LevelFields& F = c->F[l];
     double** scal[] = {&F.bulK, &F.G, &F.gc, &F.d, &F.H, &F.fd, &F.Ke, &F.Ge, &F.R, &F.dold, &F.preMd, &F.pd, &F.wd, &F.tmp1};
-    double** vec[] = {&F.u, &F.fu, &F.ru, &F.uold, &F.preMu, &F.p, &F.w, &F.z};
+    double** vec[] = {&F.u, &F.fu, &F.ru, &F.uold, &F.preMu, &F.p, &F.w, &F.tmp3};
     for (double** p : scal) {
       cudaError_t ae = cudaMalloc((void**)p, sizeof(double) * n);
       if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMalloc(level field)"));
@@ -1095,7 +1067,7 @@ int hpc_destroy(hpc_ctx* c) {
   for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
     LevelFields& F = c->F[l];
     void* ptrs[] = {F.bulK, F.G, F.gc, F.d, F.H, F.fd, F.Ke, F.Ge, F.R, F.dold, F.preMd, F.pd, F.wd, F.tmp1,
-                    F.u, F.fu, F.ru, F.uold, F.preMu, F.p, F.w, F.z, F.p2, F.choice, F.gpm};
+                    F.u, F.fu, F.ru, F.uold, F.preMu, F.p, F.w, F.tmp3, F.choice, F.gpm};
     for (void* p : ptrs)
       if (p) cudaFree(p);
   }
@@ -1158,12 +1130,6 @@ int hpc_set_tensor_apply(hpc_ctx* c, int on) {
 int hpc_set_fused_coarsest(hpc_ctx* c, int on) {
   if (!c) return arg_fail("null context");
   c->fused_coarsest = on != 0;
-  return HPC_OK;
-}
-
-int hpc_set_fused_direction(hpc_ctx* c, int on) {
-  if (!c) return arg_fail("null context");
-  c->fused_dir = on != 0;
   return HPC_OK;
 }
 
@@ -1556,21 +1522,16 @@ int hpc_phase_field(hpc_ctx* c, const hpc_mg* mg, double lc, int t, double* fd_n
   return HPC_OK;
 }
 
-int hpc_step(hpc_ctx* c, const hpc_step_params* p, double* out) {
-  if (!c || !p || !out) return arg_fail("bad argument");
+}  // extern "C"
+
+namespace hpc {
+
+// The part of an increment between the two solves (crack_propagation.cpp:71-85): the load schedule
+// at t == 0, the history update, its Voigt averages and the phase-field right-hand sides.
+int step_mid(hpc_ctx* c, const hpc_step_params* p) {
   const double U_unit = 1.0;
   const int L = c->maxlevel;
-  int rc, mcy = 0, pcy = 0;
-  long long mit = 0, pit = 0;
-  if (p->mech_solver == HPC_MECH_FCG || p->mech_solver == HPC_MECH_MIXED) {
-    if ((rc = u_entire_fcg_dev(c, p->mg_u, p->small_k, U_unit, p->t, p->mech_tol, &mcy, &mit,
-                               p->mech_solver == HPC_MECH_MIXED)))
-      return rc;
-  } else if (p->mech_solver == HPC_MECH_FAS) {
-    if ((rc = u_entire_dev(c, p->mg_u, p->small_k, U_unit, p->t, p->mech_tol, &mcy, &mit))) return rc;
-  } else {
-    return arg_fail("unknown mech_solver");
-  }
+  int rc;
   if (p->t == 0) {
     if (p->ut0 <= 0.0) {
       double ue;
@@ -1590,7 +1551,14 @@ int hpc_step(hpc_ctx* c, const hpc_step_params* p, double* out) {
   if ((rc = voigt_all_level(c, HPC_H))) return rc;
   for (int l = L; l >= 0; --l)
     if ((rc = launch_fd_h(c, l))) return rc;
-  if ((rc = phase_field_dev(c, p->mg_d, p->lc, p->pf_tol, &pcy, &pit))) return rc;
+  return HPC_OK;
+}
+
+// The end of an increment (crack_propagation.cpp:86-121): d maxima with the d_old update, the top
+// reaction sum, the next load, the step outputs.
+int step_end(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int pcy, long long pit, double* out) {
+  const double U_unit = 1.0;
+  int rc;
   if ((rc = launch_dmax(c, S_RES0, S_RES1, true))) return rc;
   if ((rc = launch_top_sum(c, S_RES2))) return rc;
   double r3[3];
@@ -1608,6 +1576,29 @@ int hpc_step(hpc_ctx* c, const hpc_step_params* p, double* out) {
   out[6] = (double)mit;
   out[7] = (double)pit;
   return HPC_OK;
+}
+
+}  // namespace hpc
+
+extern "C" {
+
+int hpc_step(hpc_ctx* c, const hpc_step_params* p, double* out) {
+  if (!c || !p || !out) return arg_fail("bad argument");
+  const double U_unit = 1.0;
+  int rc, mcy = 0, pcy = 0;
+  long long mit = 0, pit = 0;
+  if (p->mech_solver == HPC_MECH_FCG || p->mech_solver == HPC_MECH_MIXED) {
+    if ((rc = u_entire_fcg_dev(c, p->mg_u, p->small_k, U_unit, p->t, p->mech_tol, &mcy, &mit,
+                               p->mech_solver == HPC_MECH_MIXED)))
+      return rc;
+  } else if (p->mech_solver == HPC_MECH_FAS) {
+    if ((rc = u_entire_dev(c, p->mg_u, p->small_k, U_unit, p->t, p->mech_tol, &mcy, &mit))) return rc;
+  } else {
+    return arg_fail("unknown mech_solver");
+  }
+  if ((rc = step_mid(c, p))) return rc;
+  if ((rc = phase_field_dev(c, p->mg_d, p->lc, p->pf_tol, &pcy, &pit))) return rc;
+  return step_end(c, p, mcy, mit, pcy, pit, out);
 }
 
 // ---------------------------------------------------------------- material / history

@@ -37,8 +37,7 @@ struct LevelFields {
   double *u, *fu, *ru, *uold;  // 3n each; component c at +c*n
   int8_t* choice;
   // work arrays
-  double *preMu, *p, *w, *z;     // 3n; preMu holds the inverse diagonal while a solve runs; z = M^-1 r
-  double* p2;                     // finest level: second PCG direction of the fused direction update (first use)
+  double *preMu, *p, *w, *tmp3;  // 3n; preMu holds the inverse diagonal while a solve runs
   double *preMd, *pd, *wd, *tmp1;  // n;  preMd likewise
   uint8_t* bc_host_copy;           // host copies of the axis flags (nx+ny+nz bytes)
   double* gpm;  // finest level: Gauss-point moduli of the running mechanical solve, 16n (first use)
@@ -62,6 +61,9 @@ enum Scalar : int {
   S_RES1 = 4,
   S_RES2 = 5,
   S_ERR = 6,      // set to 1 by a kernel whose bounded wait ran out (tensor-core apply)
+  S_LCOUNT = 7,   // device-driven solve loops (batched steps): cycles run,
+  S_LREL = 8,     //   the convergence ratio the loop tests,
+  S_LTRUE = 9,    //   true-residual recomputations of the flexible PCG
   S_PCG = 16,     // pcg scratch: rz[-1..kMaxRelax], pw[0..kMaxRelax), rn[0..kMaxRelax)
 };
 constexpr int kMaxRelax = 4096;
@@ -85,6 +87,7 @@ inline int slot_fdummy(int k) { return S_FCG + 8 + (k & 1); }
 }  // namespace hpc
 
 struct hpc_ctx {
+  unsigned long long uid;  // unique per context of the process (keys of the batched graphs)
   hpc_geometry geo;
   int maxlevel;
   double box[6];  // xa xb ya yb za zb
@@ -119,7 +122,6 @@ struct hpc_ctx {
   int tc_apply;        // precision form: element contraction on the tensor cores (hpc_set_tensor_apply)
   int fused_coarsest;  // coarse-level pcg_u in one block when the level fits (hpc_set_fused_coarsest)
   int gpm_active;      // finest applies read F[maxlevel].gpm (set while a mechanical solve runs)
-  int fused_dir;       // finest pcg_u forms p = M^-1 r + beta p inside the apply (hpc_set_fused_direction)
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
@@ -183,10 +185,7 @@ int vtk_release(hpc_ctx* c);
 
 // ---------------------------------------------------------------- kernel launchers
 // Element operators (element_kernels.cu).  `src` is a 3n (mech) or n (pf) vector on level L.
-// EPI_PCGDIR: the PCG apply with the direction update in its staging: p = z + beta p_old formed from
-// the staged z = M^-1 r and p_old, w = K p, (p, w), p written by the node's owner (finest level,
-// precomputed Gauss-point moduli).
-enum MechEpi { EPI_PLAIN = 0, EPI_RESIDUAL = 1, EPI_PCG = 2, EPI_FAS = 3, EPI_REACTION = 4, EPI_PCGDIR = 5 };
+enum MechEpi { EPI_PLAIN = 0, EPI_RESIDUAL = 1, EPI_PCG = 2, EPI_FAS = 3, EPI_REACTION = 4 };
 
 struct MechCall {
   int level;
@@ -199,12 +198,6 @@ struct MechCall {
   double* fu;
   bool set_fnorm;     // t == 0 on the finest level (mechanical_pcg.cpp:252-258)
   const double* invM; // RESIDUAL: inverse diagonal for rz = sum r^2 invM (null: no rz)
-  double* zout;       // RESIDUAL: z = M^-1 r written here when not null
-  // PCGDIR: src = z; p = first ? z : z + beta p_old with beta = scal[s_bnum] / scal[s_bden]
-  const double* pold;
-  double* pnew;
-  int s_bnum, s_bden;
-  bool first;
   // FAS: fc = K_c u_c + full-weighting(rf)
   const double* rf;
   int fine_level;
@@ -265,9 +258,8 @@ int launch_pf_diag(hpc_ctx* c, int level, double lc, double* out);
 // nodes; scal[s_rz_next] = sum r^2/preM; scal[s_rn] = sum r^2.
 int launch_mech_update(hpc_ctx* c, int level, const double* p, int s_rz, int s_pw, int s_rz_next, int s_rn);
 // Same on explicit arrays: x += alpha p, r -= alpha w (Dirichlet rows zero), alpha = scal[s_num]/scal[s_den].
-// zout (optional): z = M^-1 r of the updated residual, for a following fused direction update.
 int launch_mech_update_on(hpc_ctx* c, int level, double* x, double* r, const double* p, const double* w,
-                          const double* invM, int s_num, int s_den, int s_rz_next, int s_rn, double* zout = nullptr);
+                          const double* invM, int s_num, int s_den, int s_rz_next, int s_rn);
 // sums (a, b) and (a, c) over a 3n vector of a level into scal[s0], scal[s1] (c may be null)
 int launch_dot2(hpc_ctx* c, int level, const double* a, const double* b, const double* cv, int s0, int s1);
 int launch_dot2(hpc_ctx* c, int level, const float* a, const double* b, const double* cv, int s0, int s1);
@@ -321,5 +313,25 @@ bool coarse_pcg_fits(hpc_ctx* c, int level);
 int coarse_pcg_prepare();
 int launch_coarse_pcg(hpc_ctx* c, int level, double Ut, int nb);
 int tuned_shapes(int* out5, int cap);  // measured strip shapes: {nx, ny, nz, wy, cz} per entry
+
+
+// ---------------------------------------------------------------- solver pieces (hpcrack.cu) shared
+// by the host-driven solves of hpc_step and the device-driven loops of hpc_batch_step
+int check_zero_diags(hpc_ctx* c, int top, const char* what);
+int mech_diags(hpc_ctx* c, int top, double small_k);
+int pf_diags(hpc_ctx* c, int top, double lc);
+int mech_material(hpc_ctx* c, double small_k);
+int gp_material(hpc_ctx* c, double small_k);
+int cycle_u_top(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, bool allow_capture);
+int cycle_d_top(hpc_ctx* c, const hpc_mg& mg, double lc, bool allow_capture);
+int ensure_f32(hpc_ctx* c);
+int f32_material(hpc_ctx* c);
+int ensure_fcg(hpc_ctx* c);
+int fcg_residual(hpc_ctx* c, double small_k, int t, int s_rn);
+int fcg_iteration(hpc_ctx* c, const hpc_mg& mg, double small_k, int k, bool mixed, bool coarse_graph);
+int voigt_all_level(hpc_ctx* c, int field);
+int step_mid(hpc_ctx* c, const hpc_step_params* p);
+int step_end(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int pcy, long long pit, double* out);
+int launch_set_scalar(hpc_ctx* c, int slot, double v);
 
 }  // namespace hpc

@@ -57,10 +57,9 @@ template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
-// z (optional): M^-1 r of the updated residual, the same products the (r, M^-1 r) sum uses.
 template <typename T>
 __global__ void mech_update_kernel(LevelGeo g, T* u, T* r, const T* p, const T* w, const T* invM, int s_rz, int s_pw,
-                                   RedTarget red, T* z) {
+                                   RedTarget red) {
   using V2 = typename Vec2<T>::type;
   const T alpha = (T)(red.scal[s_rz] / red.scal[s_pw]);
   double rz = 0.0, rn = 0.0;
@@ -95,12 +94,8 @@ __global__ void mech_update_kernel(LevelGeo g, T* u, T* r, const T* p, const T* 
       rv.y = fix[1][m] ? T(0) : fma(-wv.y, alpha, rv.y);
       *reinterpret_cast<V2*>(u + o) = uv;
       *reinterpret_cast<V2*>(r + o) = rv;
-      V2 zv;
-      zv.x = rv.x * mv.x;
-      zv.y = rv.y * mv.y;
-      if (z) *reinterpret_cast<V2*>(z + o) = zv;
-      rz = fma((double)rv.x, (double)zv.x, rz);
-      rz = fma((double)rv.y, (double)zv.y, rz);
+      rz = fma((double)rv.x, (double)(rv.x * mv.x), rz);
+      rz = fma((double)rv.y, (double)(rv.y * mv.y), rz);
       rn = fma((double)rv.x, (double)rv.x, rn);
       rn = fma((double)rv.y, (double)rv.y, rn);
     }
@@ -110,14 +105,14 @@ __global__ void mech_update_kernel(LevelGeo g, T* u, T* r, const T* p, const T* 
 }
 
 int launch_mech_update_on(hpc_ctx* c, int level, double* x, double* r, const double* p, const double* w,
-                          const double* invM, int s_num, int s_den, int s_rz_next, int s_rn, double* zout) {
+                          const double* invM, int s_num, int s_den, int s_rz_next, int s_rn) {
   const LevelGeo& g = c->L[level];
   const long long pairs = (long long)(g.px / 2) * g.ny * g.nz;
   const int grid = (int)std::min<long long>((pairs + kRowThreads - 1) / kRowThreads, (long long)num_sms_v() * 8);
   const int cls = level == c->maxlevel ? HPC_KC_MECH_UPDATE_FINEST : HPC_KC_NONE;
   timing_begin(c, cls);
   mech_update_kernel<<<grid, kRowThreads, 0, c->stream>>>(g, x, r, p, w, invM, s_num, s_den,
-                                                          make_red(c, s_rz_next, s_rn, -1), zout);
+                                                          make_red(c, s_rz_next, s_rn, -1));
   timing_end(c, cls);
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
@@ -943,7 +938,7 @@ int launch_mech_update_f32(hpc_ctx* c, int level, int s_num, int s_den, int s_rz
   const long long pairs = (long long)(g.px / 2) * g.ny * g.nz;
   const int grid = (int)std::min<long long>((pairs + kRowThreads - 1) / kRowThreads, (long long)num_sms_v() * 8);
   mech_update_kernel<float><<<grid, kRowThreads, 0, c->stream>>>(g, F.u, F.ru, F.p, F.w, F.invM, s_num, s_den,
-                                                                  make_red(c, s_rz_next, s_rn, -1), (float*)nullptr);
+                                                                  make_red(c, s_rz_next, s_rn, -1));
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
 }

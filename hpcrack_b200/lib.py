@@ -11,7 +11,8 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libhpcrack_b200.so")
+# HPCRACK_LIB selects another build of the same library (e.g. two builds timed against each other).
+LIB_PATH = os.environ.get("HPCRACK_LIB") or os.path.join(HERE, "libhpcrack_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "hpcrack.h")
 
 HPC_OK = 0
@@ -60,11 +61,13 @@ SIGNATURES = {
     "hpc_set_choice_quirk": [_ctx, _i],
     "hpc_set_autotune": [_ctx, _i],
     "hpc_set_fused_coarsest": [_ctx, _i],
-    "hpc_set_fused_direction": [_ctx, _i],
     "hpc_set_tensor_apply": [_ctx, _i],
     "hpc_tuned_shapes": [_ip, _i, _ip],
     "hpc_launch_count": [_ctx, C.POINTER(C.c_longlong), _i],
     "hpc_binary_version": [_ip],
+    "hpc_batch_create": [C.POINTER(C.c_void_p)],
+    "hpc_batch_destroy": [_vp],
+    "hpc_batch_step": [_vp, C.POINTER(C.c_void_p), _i, C.POINTER(hpc_step_params), _dp],
     "hpc_stream": [_ctx],
     "hpc_kernel_timing": [_ctx, _i],
     "hpc_kernel_time": [_ctx, C.POINTER(C.c_longlong), _dp],

@@ -77,15 +77,17 @@ def default_footprint(w: ms.Workload) -> int:
     return Hierarchy.footprint(w.maxlevel, w.element_nb, x0=w.x_start)
 
 
-def run_request(solver, w: ms.Workload, increments: int, mech_solver: int = 0, precision_mg: bool = True):
-    """One fracture run on an allocated solver: material from the image, pre-crack, increments
-    (mech_solver 0: the reference's FAS cycles, 1: flexible PCG preconditioned by one FP64 V-cycle,
-    2: the precision form; the flexible forms use solver.precision_mg's cycle unless precision_mg is
-    False)."""
+def request_mg_u(w: ms.Workload, mech_solver: int, precision_mg: bool = True):
+    """The mechanical cycle parameters of a request: the workload's for the reference's FAS cycles,
+    solver.precision_mg's preconditioner cycle for the flexible forms unless precision_mg is False."""
     from .solver import precision_mg as _precision_mg
-    mg_u = w.mg_u
     if mech_solver != 0 and precision_mg:
-        mg_u = _precision_mg(w.maxlevel, w.element_nb, w.mg_u[4])
+        return _precision_mg(w.maxlevel, w.element_nb, w.mg_u[4])
+    return w.mg_u
+
+
+def prepare_request(solver, w: ms.Workload):
+    """Material from the image and the pre-crack (image_input.cpp:120-282, strain_history.cpp:30-70)."""
     nx, ny, nz = w.nodes
     solver.image_material(w.image, (nx, ny, nz), w.table(), w.voxel_size)
     if w.crack:
@@ -93,6 +95,15 @@ def run_request(solver, w: ms.Workload, increments: int, mech_solver: int = 0, p
         solver.set(H_FIELD, w.maxlevel, Hc)
         solver.set(D_FIELD, w.maxlevel, dc)
         solver.voigt_all_level(H_FIELD)
+
+
+def run_request(solver, w: ms.Workload, increments: int, mech_solver: int = 0, precision_mg: bool = True):
+    """One fracture run on an allocated solver: material from the image, pre-crack, increments
+    (mech_solver 0: the reference's FAS cycles, 1: flexible PCG preconditioned by one FP64 V-cycle,
+    2: the precision form; the flexible forms use solver.precision_mg's cycle unless precision_mg is
+    False)."""
+    mg_u = request_mg_u(w, mech_solver, precision_mg)
+    prepare_request(solver, w)
     outs = []
     for t in range(increments):
         outs.append(solver.step(t, mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
@@ -213,6 +224,110 @@ class SolveServer:
                 if solver is not None:
                     solver.close()
                 self._release(req)
+
+
+class BatchServer(SolveServer):
+    """Continuous batching with the library's batched increments (hpc_batch_step).
+
+    One engine thread owns every admitted request's context.  Each round it admits what the HBM
+    budget and the slots allow (arrival order), then advances every active request by one increment
+    in ONE batched call: each solve phase of all requests is one CUDA graph launch whose per-request
+    loops run to their own convergence.  A request that finished its increments leaves after the
+    round, and its memory and slot go to the next waiting request.  The requests' results are the same
+    bits as run alone (hpc_batch_step's guarantee); latency counts from arrival to the end of the round
+    that completed the request.  `batch_factory` makes the batch object (hpcrack_b200.solver.Batch by
+    default; a fake in host-only tests)."""
+
+    def __init__(self, *args, batch_factory: Callable = None, **kw):
+        super().__init__(*args, **kw)
+        self.batch_factory = batch_factory
+        self.rounds = 0
+
+    def start(self):
+        self._t0 = time.perf_counter()
+        th = threading.Thread(target=self._engine, name="batch-engine", daemon=True)
+        th.start()
+        self._workers.append(th)
+
+    def _take(self, block: bool) -> list:
+        """Admits pending requests that fit (arrival order, head first); blocks for one when asked."""
+        out = []
+        with self._cv:
+            while True:
+                while self._pending and self._active < self.slots:
+                    head = self._pending[0]
+                    if self._used + head.footprint > self.budget:
+                        break
+                    self._pending.pop(0)
+                    self._used += head.footprint
+                    self._active += 1
+                    self.peak_used = max(self.peak_used, self._used)
+                    self.peak_active = max(self.peak_active, self._active)
+                    out.append(head)
+                if out or not block or (self._closed and not self._pending):
+                    return out
+                self._cv.wait()
+
+    def _engine(self):
+        from .solver import step_params
+        batch = None
+        active = []  # [request, solver, t, outputs, admitted]
+        try:
+            if self.batch_factory is None:
+                from .solver import Batch
+                batch = Batch()
+            else:
+                batch = self.batch_factory()
+            while True:
+                for req in self._take(block=not active):
+                    solver = None
+                    try:
+                        solver = self.factory(req.workload)
+                        prepare_request(solver, req.workload)
+                        active.append([req, solver, 0, [], self.now()])
+                    except BaseException as exc:
+                        self.errors[req.rid] = exc
+                        if solver is not None:
+                            solver.close()
+                        self._release(req)
+                if not active:
+                    with self._cv:
+                        if self._closed and not self._pending:
+                            return
+                    continue
+                params = []
+                for req, _, t, _, _ in active:
+                    w = req.workload
+                    params.append(step_params(t, request_mg_u(w, self.mech_solver, self.precision_mg), w.mg_d,
+                                              w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du, dU_factor=w.du_factor,
+                                              mech_tol=w.mech_tol, pf_tol=w.pf_tol, mech_solver=self.mech_solver))
+                outs = batch.step([a[1] for a in active], params)
+                self.rounds += 1
+                keep = []
+                for a, o in zip(active, outs):
+                    a[2] += 1
+                    a[3].append(o)
+                    req, solver = a[0], a[1]
+                    if a[2] < req.increments:
+                        keep.append(a)
+                        continue
+                    fields = None
+                    if self.keep_fields:
+                        L = req.workload.maxlevel
+                        fields = {"u": solver.get(16, L), "d": solver.get(D_FIELD, L), "H": solver.get(H_FIELD, L)}
+                    self.results[req.rid] = Result(req.rid, a[3], a[4], self.now(), req.arrival, fields)
+                    solver.close()  # the round's graph has completed; the next round rebuilds without it
+                    self._release(req)
+                active = keep
+        except BaseException as exc:  # reported by replay()
+            for a in active:
+                self.errors[a[0].rid] = exc
+        finally:
+            if batch is not None:
+                batch.close()
+            for a in active:
+                a[1].close()
+                self._release(a[0])
 
 
 # ------------------------------------------------------------------------------------------------

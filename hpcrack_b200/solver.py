@@ -59,6 +59,54 @@ def mg_params(mg5) -> _L.hpc_mg:
     return _L.hpc_mg(*[int(v) for v in mg5])
 
 
+def step_params(t, mg_u, mg_d, small_k, lc, voxel_size, ut0=0.0, dU=0.0, dU_factor=1.5e-3, mech_tol=1e-6,
+                pf_tol=1e-12, mech_solver=MECH_FAS) -> _L.hpc_step_params:
+    """hpc_step_params of one staggered increment (the arguments of Hierarchy.step)."""
+    return _L.hpc_step_params(int(t), mg_params(mg_u), mg_params(mg_d), small_k, lc, voxel_size, ut0, dU, dU_factor,
+                              mech_tol, pf_tol, int(mech_solver))
+
+
+class Batch:
+    """hpc_batch: one staggered increment of many specimens per call (hpc_batch_step).
+
+    Every specimen's mechanical and phase-field solve runs as a device-driven loop inside one CUDA graph
+    per batch (one launch per solve phase for all specimens, each converging at its own pace); the
+    results are the same bits as Hierarchy.step on each specimen alone."""
+
+    def __init__(self):
+        self.lib = _L.load()
+        h = C.c_void_p()
+        _L.check("hpc_batch_create", self.lib.hpc_batch_create(C.byref(h)))
+        self.h = h
+
+    def step(self, hiers, params):
+        """Advances hiers[i] by the increment params[i] (step_params); returns one 8-value output per
+        specimen, as Hierarchy.step returns."""
+        n = len(hiers)
+        ctxs = (C.c_void_p * n)(*[hh.h.value for hh in hiers])
+        ps = (_L.hpc_step_params * n)(*params)
+        out = (C.c_double * (8 * n))()
+        _L.check("hpc_batch_step", self.lib.hpc_batch_step(self.h, ctxs, n, ps, out))
+        return [list(out[8 * i:8 * i + 8]) for i in range(n)]
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hpc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class Hierarchy:
     """Device-resident multigrid hierarchy of one specimen."""
 
@@ -154,11 +202,6 @@ class Hierarchy:
     def set_fused_coarsest(self, on: bool):
         """Coarsest-level pcg_u in one thread block (default) or as per-iteration kernels."""
         self._c("hpc_set_fused_coarsest", int(bool(on)))
-
-    def set_fused_direction(self, on: bool):
-        """hpc_set_fused_direction: the finest PCG direction update inside the operator apply (1) or
-        as a pass of its own (0, default, faster on B200); the same bits either way."""
-        self._c("hpc_set_fused_direction", int(bool(on)))
 
     def set_autotune(self, on: bool):
         """Measure strip shapes on first use of each kernel and level size (see hpc_set_autotune)."""
@@ -314,8 +357,7 @@ class Hierarchy:
              pf_tol=1e-12, mech_solver=MECH_FAS):
         """One staggered increment; mech_solver MECH_FAS (the reference's V-cycles), MECH_FCG (flexible
         PCG preconditioned by one V-cycle per iteration) or MECH_MIXED (the same with the V-cycle in FP32)."""
-        p = _L.hpc_step_params(int(t), mg_params(mg_u), mg_params(mg_d), small_k, lc, voxel_size, ut0, dU, dU_factor,
-                               mech_tol, pf_tol, int(mech_solver))
+        p = step_params(t, mg_u, mg_d, small_k, lc, voxel_size, ut0, dU, dU_factor, mech_tol, pf_tol, mech_solver)
         out = (C.c_double * 8)()
         self._c("hpc_step", C.byref(p), out)
         return list(out)

@@ -132,12 +132,6 @@ int hpc_tuned_shapes(int* out5, int cap, int* count);
  * shared memory (up to about 10^3 nodes); 0 uses the per-iteration kernels.  The two differ only in
  * the order of the same sums. */
 int hpc_set_fused_coarsest(hpc_ctx* ctx, int on);
-/* No counterpart in the reference: 1 forms the PCG direction p = M^-1 r + beta p of the
- * finest-level mechanical smoother (mechanical_pcg.cpp:274-292) inside the next operator apply's
- * staging instead of in a pass of its own, while the Gauss-point moduli of a mechanical solve are
- * in use; 0 (default) keeps the separate pass.  Both compute the same products and fma: the same
- * bits.  On B200 the fused apply (twice the staged rows) costs more than the pass it saves. */
-int hpc_set_fused_direction(hpc_ctx* ctx, int on);
 /* No counterpart in the reference: 1 runs the element operator of the precision form's FP32 V-cycle
  * (mech_solver HPC_MECH_MIXED) on the tensor cores - strains and element forces as two TF32 GEMMs
  * per 128 elements (tcgen05, accumulators in tensor memory), Hooke's law per Gauss point on the
@@ -301,6 +295,25 @@ int hpc_refine_standard(hpc_ctx* ctx, int uf_field, int uc_field, int ucold_fiel
  * nodal Voigt-Reuss-Hill hierarchy (coarse_VR). */
 int hpc_image_material(hpc_ctx* ctx, const uint8_t* image, const int* voxel_n, int ngray, const int* gray,
                        const double* E, const double* nu, const double* gc, double voxel_size);
+
+/* ---------------- batched increments ---------------- */
+/* No counterpart in the reference (it runs one specimen per program): a batch advances many contexts
+ * (specimens of any sizes, on one device) by one staggered increment each - the loop body of
+ * crack_propagation.cpp:65-121, as hpc_step does for one context.  Each specimen's mechanical solve
+ * (any mech_solver) and phase-field solve is a device-driven loop: one CUDA graph per batch holds,
+ * for every specimen, a conditional WHILE node whose body is the specimen's V-cycle (or flexible-PCG
+ * iteration) and a kernel applying the reference's stopping rule, so one graph launch runs every
+ * specimen's solve to its own convergence (at most ncy cycles).  Results are bit-identical to
+ * hpc_step on each context alone.  The graphs are kept and reused while the batch's composition and
+ * the specimens' loop parameters stay the same, and rebuilt before a call with any other composition
+ * runs, so a context may be destroyed once the call that ran it has returned.  One calling thread per
+ * batch. */
+typedef struct hpc_batch hpc_batch;
+int hpc_batch_create(hpc_batch** out);
+int hpc_batch_destroy(hpc_batch* batch);
+/* ctxs[0..n): distinct contexts on one device; params[i] drives ctxs[i] (its own t, tolerances, mg
+ * parameters, mech_solver); out[8 i .. 8 i + 8) receives what hpc_step writes for ctxs[i]. */
+int hpc_batch_step(hpc_batch* batch, hpc_ctx* const* ctxs, int n, const hpc_step_params* params, double* out);
 
 /* ---------------- allocation-free variant ---------------- */
 /* No counterpart in the reference: d_max and delta_d_max (the reductions of hpc_d_max /

@@ -174,23 +174,3 @@ def test_cracked_specimen_at_benchmark_tolerance(name, steps):
         assert abs(og[2] - oo[2]) <= 1e-12 and abs(og[3] - oo[3]) <= 1e-12 * abs(oo[3]), t
     gpu.close()
     orc.close()
-
-
-@pytest.mark.parametrize("name,steps", [("crack33", 2), ("parity65", 2)])
-def test_fused_direction_update_same_bits(name, steps):
-    """The finest PCG direction update inside the operator apply (default) and as a pass of its own
-    compute the same products and fma: increments agree bit for bit."""
-    w = ms.make_workload(name)
-    L = w.maxlevel
-    res = []
-    for fused in (True, False):
-        gpu = Hierarchy(L, w.element_nb, x0=w.x_start)
-        gpu.set_fused_direction(fused)
-        load_workload([gpu], w)
-        outs = [gpu.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
-                         mech_tol=w.mech_tol, pf_tol=w.pf_tol) for t in range(steps)]
-        res.append((outs, [gpu.get(f, L) for f in (U, D, H)]))
-        gpu.close()
-    assert res[0][0] == res[1][0]
-    for a, b in zip(res[0][1], res[1][1]):
-        assert np.array_equal(a, b)

@@ -102,3 +102,45 @@ def test_hierarchy_rule():
     assert ms.hierarchy_for((257, 257, 257)) == (5, (8, 8, 8))
     assert ms.hierarchy_for((257, 129, 65)) == (3, (32, 16, 8))
     assert ms.hierarchy_for((193, 193, 193)) == (4, (12, 12, 12))
+
+
+class FakeBatch:
+    """Stands in for hpcrack_b200.solver.Batch: one call advances every given solver by its own t."""
+    sizes = []
+
+    def step(self, hiers, params):
+        FakeBatch.sizes.append(len(hiers))
+        return [h.step(p.t) for h, p in zip(hiers, params)]
+
+    def close(self):
+        pass
+
+
+def test_batch_server_rounds_admission_and_results():
+    """The batched engine: every round advances all active requests by one increment in one call;
+    requests are admitted in arrival order within the budget and slots, leave after their last
+    increment and hand their memory to the next; each result holds its own increments in order."""
+    FakeBatch.sizes = []
+    incs = [2, 3, 1, 2, 2]
+    reqs = [_req(i, 9, arrival=0.0, footprint=[40, 30, 50, 20, 60][i], increments=incs[i]) for i in range(5)]
+    srv = sv.BatchServer(hbm_budget=100, slots=3, solver_factory=FakeSolver, batch_factory=FakeBatch)
+    res = srv.replay(reqs)
+    assert [r.rid for r in res] == [0, 1, 2, 3, 4]
+    assert srv.peak_used <= 100 and srv.peak_active <= 3
+    assert FakeSolver.live == 0
+    for r, n in zip(res, incs):
+        assert [o[0] for o in r.outputs] == [float(t) for t in range(n)]
+        assert r.outputs[0][1] == float(reqs[r.rid].workload.image.sum())
+        assert r.finished >= r.admitted >= 0.0
+    assert max(FakeBatch.sizes) >= 2 and srv.rounds == len(FakeBatch.sizes)
+    assert sum(FakeBatch.sizes) == sum(incs)
+
+
+def test_batch_server_admits_late_arrivals_between_rounds():
+    FakeBatch.sizes = []
+    reqs = [_req(0, 9, arrival=0.0, increments=6), _req(1, 9, arrival=0.03, increments=2)]
+    srv = sv.BatchServer(hbm_budget=100, slots=4, solver_factory=FakeSolver, batch_factory=FakeBatch)
+    res = srv.replay(reqs)
+    assert len(res[0].outputs) == 6 and len(res[1].outputs) == 2
+    assert 2 in FakeBatch.sizes  # the late request ran in the same calls as the first one
+    assert res[1].admitted >= 0.03 - 1e-3
