@@ -75,6 +75,9 @@ def parse_args():
                          "cores (hpc_set_tensor_apply) instead of the FP32 stencil kernels")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the precision-form measurement on the same increments")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-form sub-measurement (64 specimens of the uneven-size mix, plain FAS "
+                         "against the precision form)")
     ap.add_argument("--kernel-only", type=int, default=0, metavar="NB",
                     help="profiling driver: set the specimen up, run one finest-level pcg_u with NB iterations "
                          "(NB launches of the dominant kernel) and exit")
@@ -86,6 +89,10 @@ def parse_args():
                          "admission server; prints solves/s and p50/p99 latency")
     ap.add_argument("--batch", type=int, default=0, metavar="N",
                     help="batched form: N specimens of the uneven-size mix (seeds 100..) submitted at once")
+    ap.add_argument("--cpu-plan", action="store_true",
+                    help="the reference's CPU path on this host's cores: one Internal_Force and one Fld apply on the "
+                         "65^3, 129^3 and 257^3 pre-cracked specimens, full staggered increments of the 65^3 "
+                         "configuration and of the pre-cracked 65^3 specimen, beside the same work on the GPU")
     ap.add_argument("--compare-forms", action="store_true",
                     help="run --steps increments with the plain form and with --mech-solver (default mixed) and "
                          "report solves/s of both and the per-field error against the plain run")
@@ -94,6 +101,8 @@ def parse_args():
     ap.add_argument("--requests", type=int, default=24, help="requests in a --serve sample")
     ap.add_argument("--increments", type=int, default=0, help="increments per request (default 10 serve, 5 batch)")
     ap.add_argument("--slots", type=int, default=8, help="concurrent requests on the GPU")
+    ap.add_argument("--time-graphs", action="store_true",
+                    help="batch engine: wait for each graph after its launch to time it (hpc_batch_timing)")
     ap.add_argument("--engine", choices=("batch", "threads"), default="batch",
                     help="serving / batched forms: batch = one engine thread advancing every active request by one "
                          "increment per batched call (hpc_batch_step: device-driven solve loops, one graph launch "
@@ -127,9 +136,10 @@ def run_serving(args, local):
         v = tuple(int(x) for x in args.mg_u.split(","))
         for q in reqs:
             q.workload.mg_u = v + (q.workload.mg_u[4],)
+    kw = {"time_graphs": args.time_graphs} if args.engine == "batch" else {}
     server = sv.BatchServer if args.engine == "batch" else sv.SolveServer
     srv = server(budget, args.slots, solver_factory=sv.default_factory(local),
-                 mech_solver=MECH_SOLVERS[args.mech_solver], precision_mg=not args.mg_u)
+                 mech_solver=MECH_SOLVERS[args.mech_solver], precision_mg=not args.mg_u, **kw)
     from hpcrack_b200.solver import precision_mg
     mg_used = reqs[0].workload.mg_u
     if args.mech_solver != "fas" and not args.mg_u:
@@ -150,10 +160,27 @@ def run_serving(args, local):
                                                             "mg_u": mg_used if isinstance(mg_used, str)
                                                             else list(mg_used)},
             "p50_s": st["p50_s"], "p99_s": st["p99_s"], "mean_s": st["mean_s"], "wall_s": wall,
-            "batched_calls": getattr(srv, "rounds", None),
+            "batched_calls": getattr(srv, "rounds", None), "batch_timing": getattr(srv, "batch_timing", None),
             "mdof_iter_per_s": dof_iters / wall / 1e6, "peak_active": srv.peak_active,
             "peak_hbm_gb": srv.peak_used / (1 << 30)}
     print(json.dumps(line), flush=True)
+
+
+def batch_measure(local, n=64, increments=5, mech_solver="mixed", hbm_budget_gb=150.0):
+    """The batched form: n specimens of the uneven-size mix (seeds 100..), `increments` each, submitted
+    at once to the batch engine (one engine thread; every specimen's solves as device-driven loops of
+    one CUDA graph per phase).  Returns solves/s, p50/p99 latency, wall time and the engine's timing."""
+    from hpcrack_b200 import serving as sv
+    reqs = [sv.Request(i, sv.batch_specimen(100 + i, increments), increments) for i in range(n)]
+    srv = sv.BatchServer(int(hbm_budget_gb * (1 << 30)), n, solver_factory=sv.default_factory(local),
+                         mech_solver=MECH_SOLVERS[mech_solver])
+    t0 = time.perf_counter()
+    res = srv.replay(reqs)
+    wall = time.perf_counter() - t0
+    st = sv.latency_stats(res, wall)
+    return {"solves_per_s": st["solves_per_s"], "p50_s": st["p50_s"], "p99_s": st["p99_s"], "wall_s": wall,
+            "batched_calls": srv.rounds, "peak_hbm_gb": srv.peak_used / (1 << 30),
+            "v_cycles": int(sum(o[4] for r in res for o in r.outputs))}
 
 
 def workload(args):
@@ -567,12 +594,25 @@ def run_b200(args, rank, world, local):
             forms["mixed"]["error_vs_plain"] = {k: field_errors(mixed_final[k], plain_final[k]) for k in ("u", "d", "H")}
             forms["mixed"]["error_note"] = (f"fields after increment {t_first + args.steps - 1} of both forms, each "
                                             "solved to |r|/|f| <= 1e-8; rel_l2 = |a-b|/|b|, max_abs = max|a-b|")
+    # ------------------------------------------------------------ the batched form (64-specimen mix)
+    batch = None
+    if not args.no_batch and world == 1:
+        try:
+            bp = batch_measure(local, mech_solver="fas")
+            bm = batch_measure(local, mech_solver="mixed")
+            batch = {"workload": "64 specimens, seeds 100-163, nodes per axis from {33,65,97,129,161}, inclusion "
+                                 "volume fraction in [5%,35%], 5 increments each, submitted at once",
+                     "engine": "one engine thread; each increment of all specimens is one hpc_batch_step: per solve "
+                               "phase one CUDA graph launch whose per-specimen WHILE loops run to convergence",
+                     "plain": bp, "mixed": bm, "speedup_mixed_vs_plain": bm["solves_per_s"] / bp["solves_per_s"]}
+        except Exception as exc:  # reported, never required for the headline line
+            batch = {"error": str(exc)}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": workload_config(w, world, args.mech_solver), "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cpu, "forms": forms,
+                "roofline": roofline, "cpu_baseline": cpu, "forms": forms, "batch": batch,
                 "strip_shapes": ({"autotuned": [list(x) for x in Hierarchy.tuned_shapes()]} if args.autotune
                                  else "latency model (choose_strips)"),
                 "solves_per_s": world * args.steps / (max_ms / 1e3),
@@ -629,6 +669,104 @@ def run_compare_forms(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_cpu_plan(args, local):
+    """The reference compiled from its sources (oracle/_ref), 1 rank x every host core as OpenMP
+    threads, on the benchmark's specimens: per-apply times of Internal_Force (mechanical_pcg.cpp:
+    174-191) and Fld (phase_field_pcg.cpp:93-103) with the specimen's real material, pre-crack and a
+    displacement field, and full staggered increments (crack_propagation.cpp:65-121) at the reference's
+    own thresholds, each beside the same work on the GPU."""
+    import numpy as np
+    import torch
+    from oracle import bindings as B
+    from hpcrack_b200 import microstructure as ms
+    from hpcrack_b200.solver import Hierarchy, U, D, H, RU, FD
+    torch.cuda.set_device(local)
+    cores = os.cpu_count() or 1
+    B.RefOracle._load().ref_set_threads(cores)
+    out = {"cpu_plan": True, "cores": cores, "kind": "reference", "layout": f"1 rank x {cores} OpenMP threads",
+           "applies": [], "runs": []}
+
+    def ref_for(w):
+        ref = B.RefOracle(w.maxlevel, w.element_nb, x0=w.x_start)
+        with tempfile.TemporaryDirectory() as td:
+            paths = ms.write_inputs(w, td)
+            t0 = time.perf_counter()
+            ref.input_total(td, paths["raw"], w.nodes, w.voxel_size)
+            t_in = time.perf_counter() - t0
+        if w.crack:
+            Hc, dc = ms.precrack_fields(w)
+            ref.set(H, w.maxlevel, Hc)
+            ref.set(D, w.maxlevel, dc)
+            ref.voigt_all_level(H)
+        return ref, t_in
+
+    for name in ("crack65", "mid129", "plain257"):
+        w = ms.make_workload(name)
+        L = w.maxlevel
+        gpu = load_specimen(w, local)
+        gpu.u_entire(tuple(w.mg_u[:4]) + (4,), w.small_k, 1.0, 0, 0.0)  # a displacement field of this specimen
+        u = gpu.get(U, L)
+        ref, t_in = ref_for(w)
+        ref.set(U, L, u)
+        ref.mp_choice()
+        ref.mp_all_element(w.small_k)
+        t0 = time.perf_counter()
+        ref.internal_force(L, U, RU, w.small_k)
+        t_if = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref.fld(L, D, FD, w.lc)
+        t_fld = time.perf_counter() - t0
+        gpu.mp_choice()
+        gpu.mp_all_element(w.small_k)
+        gpu.internal_force(L, U, RU, w.small_k)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(10):
+            gpu.internal_force(L, U, RU, w.small_k)
+        g_if = (time.perf_counter() - t0) / 10
+        nx, ny, nz = w.nodes
+        n = nx * ny * nz
+        out["applies"].append({"workload": name, "nodes": n, "input_total_s": t_in, "internal_force_s": t_if,
+                               "fld_s": t_fld, "internal_force_mdof_s": 3 * n / t_if / 1e6,
+                               "gpu_internal_force_s": g_if,
+                               "gpu_note": "hpc_internal_force: the nodal-form apply through the C ABI (one call, "
+                                           "host-synchronised), not the benchmark's precomputed-moduli kernel"})
+        ref.close()
+        gpu.close()
+        print(json.dumps(out["applies"][-1]), flush=True)
+
+    for name, steps in (("parity65", 3), ("crack65", 2)):
+        w = ms.make_workload(name)
+        L = w.maxlevel
+        ref, _ = ref_for(w)
+        gpu = load_specimen(w, local)
+        rec = {"workload": name, "increments": steps, "tolerance": "the reference's own: |r|^2/|f|^2 <= 1e-6, "
+                                                                    "|R|^2/|fd|^2 <= 1e-12", "cpu": [], "gpu": []}
+        for t in range(steps):
+            t0 = time.perf_counter()
+            o = ref.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du)
+            rec["cpu"].append({"t": t, "s": time.perf_counter() - t0, "mech_cycles": int(o[4]), "pf_cycles": int(o[5]),
+                               "mech_iters": int(o[6]), "pf_iters": int(o[7])})
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            og = gpu.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du)
+            rec["gpu"].append({"t": t, "s": time.perf_counter() - t0, "mech_cycles": int(og[4]),
+                               "pf_cycles": int(og[5])})
+        nx, ny, nz = w.nodes
+        n = nx * ny * nz
+        ct = sum(r["s"] for r in rec["cpu"])
+        cit = sum(3.0 * n * r["mech_iters"] + n * r["pf_iters"] for r in rec["cpu"])
+        rec["cpu_mdof_iter_per_s"] = cit / ct / 1e6
+        rec["cpu_s_per_v_cycle"] = ct / max(1, sum(r["mech_cycles"] + r["pf_cycles"] for r in rec["cpu"]))
+        rec["gpu_s"] = sum(r["s"] for r in rec["gpu"])
+        rec["cpu_s"] = ct
+        out["runs"].append(rec)
+        ref.close()
+        gpu.close()
+        print(json.dumps(rec), flush=True)
+    print(json.dumps(out), flush=True)
+
+
 def main():
     global TENSOR_APPLY
     args = parse_args()
@@ -643,6 +781,8 @@ def main():
             run_serving(args, local)
         elif args.compare_forms:
             run_compare_forms(args, local)
+        elif args.cpu_plan:
+            run_cpu_plan(args, local)
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

@@ -20,6 +20,7 @@
 // residuals are (a NaN residual fails the "not converged" comparison and ends it too).
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -194,7 +195,7 @@ int mech_pre(hpc_ctx* c, const hpc_step_params& p) {
   }
   if ((rc = launch_set_scalar(c, S_FNORM, c->f_norm))) return rc;
   if ((rc = mech_material(c, small_k))) return rc;
-  if ((rc = mech_diags(c, L, small_k))) return rc;
+  if ((rc = mech_diags_enqueue(c, L, small_k))) return rc;  // zero check after every specimen's set-up
   if (L > 0 && (rc = gp_material(c, small_k))) return rc;
   if (!fcg) {  // Initial_residual_u (mechanical_pcg.cpp:193-220)
     MechCall m{};
@@ -221,32 +222,28 @@ int mech_pre(hpc_ctx* c, const hpc_step_params& p) {
   return fcg_residual(c, small_k, p.t, slot_frn(-1));
 }
 
+// Loop scalars of a context after its solve graph: slots 0 .. S_LTRUE in one read.
+constexpr int kLoopRead = S_LTRUE + 1;
+
 // The mechanical solve after its loop: f_norm, the reactions (u_entire_dev / u_entire_fcg_dev).
-int mech_post(hpc_ctx* c, const hpc_step_params& p, int* cycles, long long* fin_iters) {
-  int rc;
+int mech_post(hpc_ctx* c, const hpc_step_params& p, const double* sc, int* cycles, long long* fin_iters) {
   const int L = c->maxlevel;
-  double s[2];
-  if ((rc = read_scalars(c, S_LCOUNT, 1, s))) return rc;
-  if ((rc = read_scalars(c, S_FNORM, 1, s + 1))) return rc;
-  *cycles = (int)s[0];
+  *cycles = (int)sc[S_LCOUNT];
   *fin_iters = (long long)*cycles * (L == 0 ? p.mg_u.nu0 : p.mg_u.nu1 + p.mg_u.nu2);
-  c->f_norm = s[1];
+  c->f_norm = sc[S_FNORM];
   LevelFields& F = c->F[L];
   if (p.mech_solver != HPC_MECH_FAS) {
-    if (p.mech_solver == HPC_MECH_MIXED && c->tc_apply) {
-      double err = 0.0;
-      if ((rc = read_scalars(c, S_ERR, 1, &err))) return rc;
-      if (err != 0.0) {
-        launch_set_scalar(c, S_ERR, 0.0);
-        set_error("tensor-core element apply: an MMA completion wait ran out");
-        return HPC_ERR_CUDA;
-      }
+    if (p.mech_solver == HPC_MECH_MIXED && c->tc_apply && sc[S_ERR] != 0.0) {
+      launch_set_scalar(c, S_ERR, 0.0);
+      set_error("tensor-core element apply: an MMA completion wait ran out");
+      return HPC_ERR_CUDA;
     }
     const size_t vbytes = sizeof(double) * 3 * (size_t)c->L[L].n;
     HPC_CUDA(cudaMemcpyAsync(F.u, c->fcg.x, vbytes, cudaMemcpyDeviceToDevice, c->stream));
     HPC_CUDA(cudaMemcpyAsync(F.fu, c->fcg.f, vbytes, cudaMemcpyDeviceToDevice, c->stream));
   }
   // externe_force_nodal (mechanical_right_hnd.cpp:18-38)
+  int rc;
   if ((rc = launch_bc(c, L, F.u, nullptr, 0, 1.0))) return rc;
   MechCall r{};
   r.level = L;
@@ -264,7 +261,7 @@ int pf_pre(hpc_ctx* c, const hpc_step_params& p) {
   int rc;
   const int L = c->maxlevel;
   if ((rc = launch_set_scalar(c, S_FDNORM, c->fd_norm))) return rc;
-  if ((rc = pf_diags(c, L, p.lc))) return rc;
+  if ((rc = pf_diags_enqueue(c, L, p.lc))) return rc;  // zero check after every specimen's set-up
   PfCall m{};  // initial_residual (phase_field_pcg.cpp:106-131)
   m.level = L;
   m.epi = EPI_RESIDUAL;
@@ -278,16 +275,11 @@ int pf_pre(hpc_ctx* c, const hpc_step_params& p) {
   return launch_pf(c, m);
 }
 
-int pf_post(hpc_ctx* c, const hpc_step_params& p, int* cycles, long long* fin_iters) {
-  int rc;
+void pf_post(hpc_ctx* c, const hpc_step_params& p, const double* sc, int* cycles, long long* fin_iters) {
   const int L = c->maxlevel;
-  double s[2];
-  if ((rc = read_scalars(c, S_LCOUNT, 1, s))) return rc;
-  if ((rc = read_scalars(c, S_FDNORM, 1, s + 1))) return rc;
-  *cycles = (int)s[0];
+  *cycles = (int)sc[S_LCOUNT];
   *fin_iters = (long long)*cycles * (L == 0 ? p.mg_d.nu0 : p.mg_d.nu1 + p.mg_d.nu2 * p.mg_d.nu2);
-  c->fd_norm = s[1];
-  return HPC_OK;
+  c->fd_norm = sc[S_FDNORM];
 }
 
 // ---------------------------------------------------------------- one specimen's loop chain
@@ -450,6 +442,11 @@ struct hpc_batch {
   cudaEvent_t done = nullptr;
   std::vector<cudaEvent_t> ready;
   int device = -1;
+  // host seconds spent (cumulative): set-up and outputs enqueued per specimen, graph builds, waits
+  // for the graphs; graph builds and launches
+  double t_host = 0.0, t_build = 0.0, t_wait = 0.0;
+  long long builds = 0, launches = 0;
+  int timing = 0;  // wait for each graph right after its launch (hpc_batch_timing)
 };
 
 namespace {
@@ -472,7 +469,9 @@ int run_phase(hpc_batch* b, int phase, hpc_ctx* const* ctxs, int n, const hpc_st
   hpc_batch::Phase& ph = b->phase[phase];
   std::vector<double> key;
   phase_key(key, ctxs, n, ps, phase);
+  auto t0 = std::chrono::steady_clock::now();
   if (!ph.exec || key != ph.key) {
+    ++b->builds;
     if (ph.exec) {
       cudaGraphExecDestroy(ph.exec);
       ph.exec = nullptr;
@@ -495,6 +494,8 @@ int run_phase(hpc_batch* b, int phase, hpc_ctx* const* ctxs, int n, const hpc_st
     }
     ph.key = key;
   }
+  b->t_build += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  ++b->launches;
   // every specimen's set-up before the graph, the graph before every specimen's next work
   for (int i = 0; i < n; ++i) {
     HPC_CUDA(cudaEventRecord(b->ready[i], ctxs[i]->stream));
@@ -503,22 +504,22 @@ int run_phase(hpc_batch* b, int phase, hpc_ctx* const* ctxs, int n, const hpc_st
   HPC_CUDA(cudaGraphLaunch(ph.exec, b->stream));
   HPC_CUDA(cudaEventRecord(b->done, b->stream));
   for (int i = 0; i < n; ++i) HPC_CUDA(cudaStreamWaitEvent(ctxs[i]->stream, b->done, 0));
+  if (b->timing) {  // instrumentation: the graph's own duration on the host clock
+    const auto w0 = std::chrono::steady_clock::now();
+    HPC_CUDA(cudaEventSynchronize(b->done));
+    b->t_wait += std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+  }
   return HPC_OK;
 }
 
-// Kernels the phase's graph ran for specimen i (instrumentation).
-int count_launches(hpc_batch* b, int phase, int i, hpc_ctx* c) {
+// Kernels the phase's graph ran for specimen i (instrumentation), from its loop scalars.
+void count_launches(hpc_batch* b, int phase, int i, hpc_ctx* c, const double* sc) {
   const ChainCount& k = b->phase[phase].counts[i];
-  double s[2];
-  int rc;
-  if ((rc = read_scalars(c, S_LCOUNT, 1, s))) return rc;
-  if ((rc = read_scalars(c, S_LTRUE, 1, s + 1))) return rc;
-  const long long runs = (long long)s[0];
-  long long n = k.fixed + (long long)s[1] * k.truer;
+  const long long runs = (long long)sc[S_LCOUNT];
+  long long n = k.fixed + (long long)sc[S_LTRUE] * k.truer;
   if (k.first) n += runs > 0 ? k.first + (runs - 1) * k.body : 0;
   else n += runs * k.body;
   c->launches += n;
-  return HPC_OK;
 }
 
 }  // namespace
@@ -554,6 +555,8 @@ int hpc_batch_destroy(hpc_batch* b) {
   delete b;
   return HPC_OK;
 }
+
+static int hpc_batch_step_body(hpc_batch* b, hpc_ctx* const* ctxs, int n, const hpc_step_params* ps, double* out);
 
 int hpc_batch_step(hpc_batch* b, hpc_ctx* const* ctxs, int n, const hpc_step_params* ps, double* out) {
   if (!b || !ctxs || !ps || !out || n < 1) {
@@ -591,17 +594,50 @@ int hpc_batch_step(hpc_batch* b, hpc_ctx* const* ctxs, int n, const hpc_step_par
     HPC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     b->ready.push_back(e);
   }
+  const auto h0 = std::chrono::steady_clock::now();
+  const double inner0 = b->t_build + b->t_wait;
+  int rc = hpc_batch_step_body(b, ctxs, n, ps, out);
+  b->t_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count() - (b->t_build + b->t_wait - inner0);
+  return rc;
+}
+
+/* Cumulative instrumentation of a batch: out[0] host seconds outside graph builds and waits, out[1]
+ * seconds building graphs, out[2] seconds waiting for graphs (measured only with waits on), out[3]
+ * graph builds, out[4] graph launches.  on >= 0 turns the per-launch wait on (1) or off (0). */
+int hpc_batch_timing(hpc_batch* b, int on, double* out) {
+  if (!b) {
+    set_error("null batch");
+    return HPC_ERR_ARG;
+  }
+  if (on >= 0) b->timing = on != 0;
+  if (out) {
+    out[0] = b->t_host;
+    out[1] = b->t_build;
+    out[2] = b->t_wait;
+    out[3] = (double)b->builds;
+    out[4] = (double)b->launches;
+  }
+  return HPC_OK;
+}
+
+static int hpc_batch_step_body(hpc_batch* b, hpc_ctx* const* ctxs, int n, const hpc_step_params* ps, double* out) {
   int rc;
   std::vector<int> mcy(n), pcy(n);
   std::vector<long long> mit(n), pit(n);
+  std::vector<double> sc((size_t)n * kLoopRead);
+  // Each stage is enqueued for every specimen before any host read, so that one specimen's read does
+  // not hold back the next specimen's work.
   // mechanical solves: set-up per specimen, every loop in one graph launch, reactions per specimen
   for (int i = 0; i < n; ++i)
     if ((rc = mech_pre(ctxs[i], ps[i]))) return rc;
+  for (int i = 0; i < n; ++i)
+    if ((rc = check_zero_diags(ctxs[i], ctxs[i]->maxlevel, "PreM_u"))) return rc;
   for (int i = 0; i < n; ++i) ctxs[i]->gpm_active = ctxs[i]->maxlevel > 0 ? 1 : 0;
   rc = run_phase(b, 0, ctxs, n, ps);
   for (int i = 0; i < n && !rc; ++i) {
-    rc = mech_post(ctxs[i], ps[i], &mcy[i], &mit[i]);
-    if (!rc) rc = count_launches(b, 0, i, ctxs[i]);
+    rc = read_scalars(ctxs[i], 0, kLoopRead, &sc[(size_t)i * kLoopRead]);
+    if (!rc) rc = mech_post(ctxs[i], ps[i], &sc[(size_t)i * kLoopRead], &mcy[i], &mit[i]);
+    if (!rc) count_launches(b, 0, i, ctxs[i], &sc[(size_t)i * kLoopRead]);
   }
   for (int i = 0; i < n; ++i) ctxs[i]->gpm_active = 0;
   if (rc) return rc;
@@ -610,12 +646,17 @@ int hpc_batch_step(hpc_batch* b, hpc_ctx* const* ctxs, int n, const hpc_step_par
     if ((rc = step_mid(ctxs[i], &ps[i]))) return rc;
     if ((rc = pf_pre(ctxs[i], ps[i]))) return rc;
   }
+  for (int i = 0; i < n; ++i)
+    if ((rc = check_zero_diags(ctxs[i], ctxs[i]->maxlevel, "Precondition_M"))) return rc;
   if ((rc = run_phase(b, 1, ctxs, n, ps))) return rc;
   for (int i = 0; i < n; ++i) {
-    if ((rc = pf_post(ctxs[i], ps[i], &pcy[i], &pit[i]))) return rc;
-    if ((rc = count_launches(b, 1, i, ctxs[i]))) return rc;
-    if ((rc = step_end(ctxs[i], &ps[i], mcy[i], mit[i], pcy[i], pit[i], out + 8 * i))) return rc;
+    if ((rc = read_scalars(ctxs[i], 0, kLoopRead, &sc[(size_t)i * kLoopRead]))) return rc;
+    pf_post(ctxs[i], ps[i], &sc[(size_t)i * kLoopRead], &pcy[i], &pit[i]);
+    count_launches(b, 1, i, ctxs[i], &sc[(size_t)i * kLoopRead]);
+    if ((rc = step_end_enqueue(ctxs[i]))) return rc;
   }
+  for (int i = 0; i < n; ++i)
+    if ((rc = step_end_finish(ctxs[i], &ps[i], mcy[i], mit[i], pcy[i], pit[i], out + 8 * i))) return rc;
   return HPC_OK;
 }
 

@@ -197,23 +197,32 @@ int check_zero_diags(hpc_ctx* c, int top, const char* what) {
 }
 
 // diag K(d) of every level 0..top into preMu; fails like the reference on a zero entry.
-int mech_diags(hpc_ctx* c, int top, double small_k) {
+// The diagonals without the zero check (check_zero_diags reads the counts: a host synchronisation).
+int mech_diags_enqueue(hpc_ctx* c, int top, double small_k) {
   for (int l = 0; l <= top; ++l) {
     int rc = launch_mech_diag(c, l, is_finest(c, l), small_k, c->F[l].preMu);
     if (rc) return rc;
     if ((rc = launch_zero_count(c, l, 3, c->F[l].preMu, S_ZEROS + l))) return rc;
     if ((rc = launch_invert(c, l, 3, c->F[l].preMu))) return rc;
   }
-  return check_zero_diags(c, top, "PreM_u");
+  return HPC_OK;
 }
-int pf_diags(hpc_ctx* c, int top, double lc) {
+int pf_diags_enqueue(hpc_ctx* c, int top, double lc) {
   for (int l = 0; l <= top; ++l) {
     int rc = launch_pf_diag(c, l, lc, c->F[l].preMd);
     if (rc) return rc;
     if ((rc = launch_zero_count(c, l, 1, c->F[l].preMd, S_ZEROS + l))) return rc;
     if ((rc = launch_invert(c, l, 1, c->F[l].preMd))) return rc;
   }
-  return check_zero_diags(c, top, "Precondition_M");
+  return HPC_OK;
+}
+int mech_diags(hpc_ctx* c, int top, double small_k) {
+  const int rc = mech_diags_enqueue(c, top, small_k);
+  return rc ? rc : check_zero_diags(c, top, "PreM_u");
+}
+int pf_diags(hpc_ctx* c, int top, double lc) {
+  const int rc = pf_diags_enqueue(c, top, lc);
+  return rc ? rc : check_zero_diags(c, top, "Precondition_M");
 }
 
 // pcg_u (mechanical_pcg.cpp:223-330) with preMu of level l already built.  Device scalars only.
@@ -1556,11 +1565,18 @@ int step_mid(hpc_ctx* c, const hpc_step_params* p) {
 
 // The end of an increment (crack_propagation.cpp:86-121): d maxima with the d_old update, the top
 // reaction sum, the next load, the step outputs.
-int step_end(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int pcy, long long pit, double* out) {
-  const double U_unit = 1.0;
+int step_end_enqueue(hpc_ctx* c) {
   int rc;
   if ((rc = launch_dmax(c, S_RES0, S_RES1, true))) return rc;
-  if ((rc = launch_top_sum(c, S_RES2))) return rc;
+  return launch_top_sum(c, S_RES2);
+}
+int step_end(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int pcy, long long pit, double* out) {
+  const int rc = step_end_enqueue(c);
+  return rc ? rc : step_end_finish(c, p, mcy, mit, pcy, pit, out);
+}
+int step_end_finish(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int pcy, long long pit, double* out) {
+  const double U_unit = 1.0;
+  int rc;
   double r3[3];
   if ((rc = read_scalars(c, S_RES0, 3, r3))) return rc;
   const double FeW = r3[2] * p->voxel_size;

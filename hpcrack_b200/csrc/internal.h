@@ -320,6 +320,8 @@ int tuned_shapes(int* out5, int cap);  // measured strip shapes: {nx, ny, nz, wy
 int check_zero_diags(hpc_ctx* c, int top, const char* what);
 int mech_diags(hpc_ctx* c, int top, double small_k);
 int pf_diags(hpc_ctx* c, int top, double lc);
+int mech_diags_enqueue(hpc_ctx* c, int top, double small_k);
+int pf_diags_enqueue(hpc_ctx* c, int top, double lc);
 int mech_material(hpc_ctx* c, double small_k);
 int gp_material(hpc_ctx* c, double small_k);
 int cycle_u_top(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, bool allow_capture);
@@ -332,6 +334,8 @@ int fcg_iteration(hpc_ctx* c, const hpc_mg& mg, double small_k, int k, bool mixe
 int voigt_all_level(hpc_ctx* c, int field);
 int step_mid(hpc_ctx* c, const hpc_step_params* p);
 int step_end(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int pcy, long long pit, double* out);
+int step_end_enqueue(hpc_ctx* c);
+int step_end_finish(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int pcy, long long pit, double* out);
 int launch_set_scalar(hpc_ctx* c, int slot, double v);
 
 }  // namespace hpc

@@ -68,6 +68,7 @@ SIGNATURES = {
     "hpc_batch_create": [C.POINTER(C.c_void_p)],
     "hpc_batch_destroy": [_vp],
     "hpc_batch_step": [_vp, C.POINTER(C.c_void_p), _i, C.POINTER(hpc_step_params), _dp],
+    "hpc_batch_timing": [_vp, _i, _dp],
     "hpc_stream": [_ctx],
     "hpc_kernel_timing": [_ctx, _i],
     "hpc_kernel_time": [_ctx, C.POINTER(C.c_longlong), _dp],

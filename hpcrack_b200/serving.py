@@ -238,10 +238,12 @@ class BatchServer(SolveServer):
     that completed the request.  `batch_factory` makes the batch object (hpcrack_b200.solver.Batch by
     default; a fake in host-only tests)."""
 
-    def __init__(self, *args, batch_factory: Callable = None, **kw):
+    def __init__(self, *args, batch_factory: Callable = None, time_graphs: bool = False, **kw):
         super().__init__(*args, **kw)
         self.batch_factory = batch_factory
+        self.time_graphs = time_graphs
         self.rounds = 0
+        self.batch_timing = None
 
     def start(self):
         self._t0 = time.perf_counter()
@@ -276,6 +278,8 @@ class BatchServer(SolveServer):
             if self.batch_factory is None:
                 from .solver import Batch
                 batch = Batch()
+                if self.time_graphs:
+                    batch.timing(True)
             else:
                 batch = self.batch_factory()
             while True:
@@ -324,6 +328,8 @@ class BatchServer(SolveServer):
                 self.errors[a[0].rid] = exc
         finally:
             if batch is not None:
+                if hasattr(batch, "timing"):
+                    self.batch_timing = batch.timing()
                 batch.close()
             for a in active:
                 a[1].close()

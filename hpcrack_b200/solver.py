@@ -89,6 +89,13 @@ class Batch:
         _L.check("hpc_batch_step", self.lib.hpc_batch_step(self.h, ctxs, n, ps, out))
         return [list(out[8 * i:8 * i + 8]) for i in range(n)]
 
+    def timing(self, on=None) -> dict:
+        """hpc_batch_timing: cumulative host seconds (enqueue/read, graph builds, graph waits when
+        on) and counts of graph builds and launches; on=True/False switches the per-launch wait."""
+        out = (C.c_double * 5)()
+        _L.check("hpc_batch_timing", self.lib.hpc_batch_timing(self.h, -1 if on is None else int(bool(on)), out))
+        return {"host_s": out[0], "build_s": out[1], "wait_s": out[2], "builds": int(out[3]), "launches": int(out[4])}
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.hpc_batch_destroy(self.h)

@@ -314,6 +314,12 @@ int hpc_batch_destroy(hpc_batch* batch);
 /* ctxs[0..n): distinct contexts on one device; params[i] drives ctxs[i] (its own t, tolerances, mg
  * parameters, mech_solver); out[8 i .. 8 i + 8) receives what hpc_step writes for ctxs[i]. */
 int hpc_batch_step(hpc_batch* batch, hpc_ctx* const* ctxs, int n, const hpc_step_params* params, double* out);
+/* No counterpart in the reference: cumulative instrumentation of a batch - out[0] host seconds spent
+ * enqueuing and reading outside graph builds and waits, out[1] seconds building graphs, out[2]
+ * seconds waiting for the graphs (only measured while waits are on), out[3] graph builds, out[4]
+ * graph launches.  on = 1 makes every hpc_batch_step wait for each graph right after its launch (to
+ * time it), 0 turns that off, -1 leaves it as it is; out may be null. */
+int hpc_batch_timing(hpc_batch* batch, int on, double* out);
 
 /* ---------------- allocation-free variant ---------------- */
 /* No counterpart in the reference: d_max and delta_d_max (the reductions of hpc_d_max /
