@@ -84,15 +84,19 @@ def parse_args():
     ap.add_argument("--profile-cycles", type=int, default=0, metavar="K",
                     help="profiling driver: set the specimen up and run two increments capped at K mechanical "
                          "and K phase-field V-cycles each (the step's kernel mix in a bounded launch count)")
-    ap.add_argument("--serve", type=float, default=0.0, metavar="RATE",
+    ap.add_argument("--serve", default="", metavar="RATE[,RATE...]",
                     help="serving form: Poisson arrivals at RATE requests/s (seed 7) through the continuous-"
-                         "admission server; prints solves/s and p50/p99 latency")
+                         "admission server; prints solves/s and p50/p99 latency, one line per rate (the same "
+                         "requests at every rate)")
     ap.add_argument("--batch", type=int, default=0, metavar="N",
                     help="batched form: N specimens of the uneven-size mix (seeds 100..) submitted at once")
     ap.add_argument("--cpu-plan", action="store_true",
                     help="the reference's CPU path on this host's cores: one Internal_Force and one Fld apply on the "
                          "65^3, 129^3 and 257^3 pre-cracked specimens, full staggered increments of the 65^3 "
                          "configuration and of the pre-cracked 65^3 specimen, beside the same work on the GPU")
+    ap.add_argument("--reference-tol", type=float, default=0.0, metavar="SQ",
+                    help="--compare-forms: also solve every increment with the FP64 flexible PCG to the squared "
+                         "ratio SQ (e.g. 1e-24) and report both forms' errors against that converged field")
     ap.add_argument("--compare-forms", action="store_true",
                     help="run --steps increments with the plain form and with --mech-solver (default mixed) and "
                          "report solves/s of both and the per-field error against the plain run")
@@ -124,13 +128,20 @@ def run_serving(args, local):
         metric, form = "solves/s", f"batched: {args.batch} specimens (seeds 100..{99 + args.batch}), sizes per axis " \
                                    f"from {{33,65,97,129,161}}, {inc} increments each, submitted at t=0"
     else:
+        rates = [float(r) for r in str(args.serve).split(",") if r]
+        if len(rates) > 1:
+            for r in rates:
+                sub = argparse.Namespace(**vars(args))
+                sub.serve = str(r)
+                run_serving(sub, local)
+            return
         inc = args.increments or 10
         kw = {}
         if args.sizes:
             kw = {"sizes": tuple((int(n),) * 3 for n in args.sizes.split(",")), "weights": None}
             kw["weights"] = tuple(1.0 for _ in kw["sizes"])
-        reqs = sv.serve_mix(args.requests, args.serve, seed=7, increments=inc, **kw)
-        metric, form = "solves/s", f"served: {args.requests} requests, Poisson arrivals at {args.serve}/s (seed 7), " \
+        reqs = sv.serve_mix(args.requests, rates[0], seed=7, increments=inc, **kw)
+        metric, form = "solves/s", f"served: {args.requests} requests, Poisson arrivals at {rates[0]}/s (seed 7), " \
                                    f"{inc} increments each"
     if args.mg_u:
         v = tuple(int(x) for x in args.mg_u.split(","))
@@ -642,30 +653,48 @@ def run_compare_forms(args, local):
     torch.cuda.set_device(local)
     w = workload(args)
     res = {}
-    for name in ("fas", args.mech_solver if args.mech_solver != "fas" else "mixed"):
+    names = ["fas", args.mech_solver if args.mech_solver != "fas" else "mixed"]
+    if args.reference_tol > 0:
+        names.append("reference")
+    for name in names:
         hier = load_specimen(w, local)
+        solver_id = MECH_SOLVERS["fcg"] if name == "reference" else MECH_SOLVERS[name]
+        tol = args.reference_tol if name == "reference" else w.mech_tol
+        mg_u = w.mg_u
+        if name != "fas":
+            from hpcrack_b200.solver import precision_mg
+            mg_u = precision_mg(w.maxlevel, w.element_nb, w.mg_u[4])
         stream = torch.cuda.ExternalStream(hier.stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
-        outs = [hier.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
-                          dU_factor=w.du_factor, mech_tol=w.mech_tol, pf_tol=w.pf_tol,
-                          mech_solver=MECH_SOLVERS[name]) for t in range(args.steps)]
+        outs = [hier.step(t, mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du,
+                          dU_factor=w.du_factor, mech_tol=tol, pf_tol=w.pf_tol,
+                          mech_solver=solver_id) for t in range(args.steps)]
         e1.record(stream)
         torch.cuda.synchronize()
         ms_tot = e0.elapsed_time(e1)
         res[name] = {"outs": outs, "ms": ms_tot, "fields": {k: hier.get(f, w.maxlevel) for k, f in
                                                               (("u", U), ("d", D), ("H", H))}}
         hier.close()
-    plain, other = res["fas"], res[[k for k in res if k != "fas"][0]]
+    form_name = names[1]
+    plain, other = res["fas"], res[form_name]
     errs = {k: field_errors(other["fields"][k], plain["fields"][k]) for k in ("u", "d", "H")}
-    line = {"metric": "solves/s", "workload": w.name, "increments": args.steps,
+    ncy = w.mg_u[4]
+    line = {"metric": "solves/s", "workload": w.name, "increments": args.steps, "mech_tol_sq": w.mech_tol,
             "plain": {"solves_per_s": args.steps / (plain["ms"] / 1e3), "ms": plain["ms"],
-                      "v_cycles": [int(o[4]) for o in plain["outs"]]},
-            "form": {"name": [k for k in res if k != "fas"][0], "solves_per_s": args.steps / (other["ms"] / 1e3),
+                      "v_cycles": [int(o[4]) for o in plain["outs"]],
+                      "hit_cycle_cap": [int(o[4]) >= ncy for o in plain["outs"]]},
+            "form": {"name": form_name, "solves_per_s": args.steps / (other["ms"] / 1e3),
                      "ms": other["ms"], "v_cycles": [int(o[4]) for o in other["outs"]]},
             "speedup": plain["ms"] / other["ms"], "field_error_vs_plain": errs,
             "reaction_rel_diff": [abs(a[1] - b[1]) / abs(b[1]) for a, b in zip(other["outs"], plain["outs"])]}
+    if "reference" in res:
+        ref = res["reference"]
+        line["reference"] = {"what": f"FP64 flexible PCG to |r|^2/|f|^2 <= {args.reference_tol:g} on every increment",
+                             "ms": ref["ms"], "v_cycles": [int(o[4]) for o in ref["outs"]]}
+        line["plain_error_vs_reference"] = {k: field_errors(plain["fields"][k], ref["fields"][k]) for k in ("u", "d", "H")}
+        line["form_error_vs_reference"] = {k: field_errors(other["fields"][k], ref["fields"][k]) for k in ("u", "d", "H")}
     print(json.dumps(line), flush=True)
 
 
@@ -777,7 +806,7 @@ def main():
             run_kernel_only(args, local)
         elif args.profile_cycles:
             run_profile_cycles(args, local)
-        elif args.serve or args.batch:
+        elif (args.serve and any(float(r) > 0 for r in str(args.serve).split(",") if r)) or args.batch:
             run_serving(args, local)
         elif args.compare_forms:
             run_compare_forms(args, local)

@@ -361,14 +361,16 @@ def batch_specimen(seed: int, increments: int = 5, maxlevel: int = 3) -> ms.Work
 def serve_mix(n: int, rate: float, seed: int = 7, increments: int = 10, sizes=SERVE_SIZES,
               weights=SERVE_WEIGHTS) -> list[Request]:
     """Poisson arrivals at `rate` requests/s; sizes drawn with `weights`; volume fraction in
-    [5 %, 35 %]."""
+    [5 %, 35 %].  Sizes and volume fractions come from one random stream and the arrival gaps from
+    another (both seeded by `seed`), so every rate serves the same requests."""
     rng = np.random.default_rng(seed)
+    arr = np.random.default_rng([seed, 1])
     t = 0.0
     reqs = []
     w = np.asarray(weights, dtype=np.float64)
     w = w / w.sum()
     for i in range(n):
-        t += float(rng.exponential(1.0 / rate))
+        t += float(arr.exponential(1.0 / rate))
         nodes = sizes[int(rng.choice(len(sizes), p=w))]
         vf = float(rng.uniform(0.05, 0.35))
         wl = ms.inclusion_workload(f"req{i}", nodes, seed * 100000 + i, vf, None, increments)

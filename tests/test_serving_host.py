@@ -89,6 +89,9 @@ def test_latency_stats_and_mixes():
     assert set(sizes) <= set(sv.SERVE_SIZES)
     again = sv.serve_mix(50, rate=20.0, seed=7, increments=10)
     assert [r.workload.nodes for r in again] == sizes
+    other_rate = sv.serve_mix(50, rate=5.0, seed=7, increments=10)  # the same requests at every rate
+    assert [r.workload.nodes for r in other_rate] == sizes
+    assert np.array_equal(other_rate[3].workload.image, reqs[3].workload.image)
     b = sv.batch_specimen(100)
     assert all(n in sv.BATCH_SIZES for n in b.nodes)
     assert all(e << b.maxlevel == n - 1 for e, n in zip(b.element_nb, b.nodes))
