@@ -64,6 +64,8 @@ def parse_args():
     ap.add_argument("--mech-solver", choices=("fas", "fcg", "mixed"), default="fas",
                     help="fas: the reference's FAS V-cycles (plain form); fcg: flexible PCG preconditioned by one "
                          "FP64 V-cycle per iteration; mixed: the precision form (FP32 V-cycle, FP64 outer PCG)")
+    ap.add_argument("--tma", action="store_true",
+                    help="stage the finest applies' node rows with tensor copies (hpc_set_tma_staging)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-timing", action="store_true")
@@ -406,6 +408,7 @@ def workload_config(w, world, mech_solver="fas"):
 
 
 TENSOR_APPLY = False  # --tensor-apply
+TMA_STAGING = False   # --tma
 
 
 def load_specimen(w, device):
@@ -414,6 +417,8 @@ def load_specimen(w, device):
     hier = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start, device=device)
     if TENSOR_APPLY:
         hier.set_tensor_apply(True)
+    if TMA_STAGING:
+        hier.set_tma_staging(True)
     hier.image_material(w.image, w.nodes, w.table(), w.voxel_size)
     if w.crack:
         Hc, dc = ms.precrack_fields(w)
@@ -797,9 +802,10 @@ def run_cpu_plan(args, local):
 
 
 def main():
-    global TENSOR_APPLY
+    global TENSOR_APPLY, TMA_STAGING
     args = parse_args()
     TENSOR_APPLY = args.tensor_apply
+    TMA_STAGING = args.tma
     rank, world, local = dist_setup()
     try:
         if args.kernel_only:

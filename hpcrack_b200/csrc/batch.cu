@@ -232,10 +232,15 @@ int mech_post(hpc_ctx* c, const hpc_step_params& p, const double* sc, int* cycle
   *fin_iters = (long long)*cycles * (L == 0 ? p.mg_u.nu0 : p.mg_u.nu1 + p.mg_u.nu2);
   c->f_norm = sc[S_FNORM];
   LevelFields& F = c->F[L];
+  if (p.mech_solver == HPC_MECH_FAS && sc[S_ERR] != 0.0) {
+    launch_set_scalar(c, S_ERR, 0.0);
+    set_error("a bounded wait in a kernel (tensor copy) ran out");
+    return HPC_ERR_CUDA;
+  }
   if (p.mech_solver != HPC_MECH_FAS) {
-    if (p.mech_solver == HPC_MECH_MIXED && c->tc_apply && sc[S_ERR] != 0.0) {
+    if (sc[S_ERR] != 0.0) {
       launch_set_scalar(c, S_ERR, 0.0);
-      set_error("tensor-core element apply: an MMA completion wait ran out");
+      set_error("a bounded wait in a kernel (tensor copy or MMA completion) ran out");
       return HPC_ERR_CUDA;
     }
     const size_t vbytes = sizeof(double) * 3 * (size_t)c->L[L].n;
@@ -460,7 +465,7 @@ void phase_key(std::vector<double>& key, hpc_ctx* const* ctxs, int n, const hpc_
     const double v[] = {(double)c->uid, (double)mg.nu0, (double)mg.nu1, (double)mg.nu2, (double)mg.gamma,
                         (double)mg.ncy, phase == 0 ? p.small_k : p.lc, phase == 0 ? p.mech_tol : p.pf_tol,
                         (double)(p.t == 0), (double)(phase == 0 ? p.mech_solver : 0), (double)c->tc_apply,
-                        (double)c->fused_coarsest, (double)c->maxlevel};
+                        (double)c->fused_coarsest, (double)c->tma_stage, (double)c->maxlevel};
     key.insert(key.end(), v, v + sizeof(v) / sizeof(v[0]));
   }
 }

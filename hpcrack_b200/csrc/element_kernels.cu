@@ -14,7 +14,9 @@
 // Every node is written once, by the warp whose output range owns it, with a fixed summation
 // order: no atomics, no block-wide barriers, deterministic results.  Warps stride over the strip
 // list (persistent grid).
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <mutex>
@@ -119,8 +121,97 @@ struct Stream {
     }
     cp_async_commit();
   }
+  // Row s has landed for every lane of the warp (this lane's copies, then the warp barrier).
+  __device__ __forceinline__ bool wait(int) const {
+    cp_async_wait2();
+    __syncwarp();
+    return true;
+  }
   __device__ __forceinline__ T at(int s, int f, int c, int col) const {
     return ring[(((s & (kRing - 1)) * NF + f) * 2 + c) * kRowW + col];
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// TMA staging (cp.async.bulk.tensor): one elected lane per warp copies a whole staged row - the 3
+// vector components on the two planes kk, kk+1, x from xs to xs + BX - 1 - with one tensor copy into
+// the warp's ring slot, completion counted on the slot's mbarrier; every lane waits on the barrier's
+// phase.  The copy's x start must be a multiple of 16 bytes, so it starts at xs = the strip's first
+// column (x0 - 1) rounded down to 16 bytes, the box is BX wide (33 columns plus that offset, rounded
+// up to 16 bytes) and the lanes index from the offset.  Out-of-range coordinates (x < 0, x >= px,
+// y = -1 or ny, z = -1 or nz) read zeros, as the cp.async staging's zero fill does; columns nx .. px-1
+// are padding slots, zero in every vector.  Loads only, no multicast, this GPU's own memory.
+// ------------------------------------------------------------------------------------------
+template <typename T> struct TmaShape;
+template <> struct TmaShape<float> { static constexpr int BX = 36; };   // 144 B; offset <= 3
+template <> struct TmaShape<double> { static constexpr int BX = 34; };  // 272 B; offset <= 1
+template <typename T>
+constexpr int tma_slot_bytes() { return ((3 * 2 * TmaShape<T>::BX * (int)sizeof(T)) + 127) / 128 * 128; }
+constexpr int kTmaHead = 128;              // per warp: 4 mbarriers, padded to the slots' 128-B alignment
+constexpr unsigned kTmaWaitPolls = 1u << 24;  // far above any copy's latency; then the kernel reports
+template <typename T>
+__host__ __device__ constexpr size_t tma_warp_bytes(int wy) {
+  return (size_t)kTmaHead + (size_t)kRing * tma_slot_bytes<T>() + (size_t)(wy - 1) * 3 * 32 * sizeof(T);
+}
+
+// The copy's inner extent is a multiple of 16 bytes and covers 33 columns after any offset below 16
+// bytes; ring slots and every warp's share of shared memory stay on 128-byte boundaries.
+static_assert(TmaShape<float>::BX * 4 % 16 == 0 && TmaShape<float>::BX >= 33 + 3, "float box");
+static_assert(TmaShape<double>::BX * 8 % 16 == 0 && TmaShape<double>::BX >= 33 + 1, "double box");
+static_assert(tma_warp_bytes<float>(2) % 128 == 0 && tma_warp_bytes<float>(4) % 128 == 0 &&
+                  tma_warp_bytes<float>(8) % 128 == 0, "float warp share");
+static_assert(tma_warp_bytes<double>(2) % 128 == 0 && tma_warp_bytes<double>(4) % 128 == 0 &&
+                  tma_warp_bytes<double>(8) % 128 == 0, "double warp share");
+static_assert(kWY == 8, "the warp-share alignment above is checked for strip heights 2, 4 and 8");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+template <typename T>
+struct TmaStream {
+  static constexpr int BX = TmaShape<T>::BX;
+  static constexpr int SLOT = tma_slot_bytes<T>() / (int)sizeof(T);  // elements per ring slot
+  T* ring;
+  uint64_t* bars;
+  const CUtensorMap* map;
+  int xs, off, y0, z0, nlayers, total, rows;
+  unsigned base;  // rows this warp staged before the strip: the slot and phase of row s are base + s's
+  double* err;
+
+  __device__ __forceinline__ void issue(int s, int lane) const {
+    if (lane != 0 || s >= total) return;
+    const int li = s / rows, r = s - li * rows;
+    const int kk = z0 - 1 + li, y = y0 - 1 + r;
+    const unsigned g = base + (unsigned)s;
+    const uint32_t bar = smem_u32(bars + (g & (kRing - 1)));
+    const uint32_t dst = smem_u32(ring + (size_t)(g & (kRing - 1)) * SLOT);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(3 * 2 * BX * (int)sizeof(T))
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(dst),
+        "l"(map), "r"(xs), "r"(y), "r"(kk), "r"(0), "r"(bar)
+        : "memory");
+  }
+  // Waits for row s; a wait that runs out sets *err and returns false (the kernel then stops).
+  __device__ __forceinline__ bool wait(int s) const {
+    const unsigned g = base + (unsigned)s;
+    const uint32_t bar = smem_u32(bars + (g & (kRing - 1)));
+    const uint32_t parity = (g / kRing) & 1u;
+    for (unsigned i = 0; i < kTmaWaitPolls; ++i) {
+      uint32_t ok;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}\n"
+          : "=r"(ok)
+          : "r"(bar), "r"(parity)
+          : "memory");
+      if (ok) return true;
+    }
+    if (err) *err = 1.0;
+    return false;
+  }
+  __device__ __forceinline__ T at(int s, int f, int c, int col) const {
+    return ring[(size_t)((base + (unsigned)s) & (kRing - 1)) * SLOT + (f * 2 + c) * BX + off + col];
   }
 };
 
@@ -142,7 +233,8 @@ struct MechKT {
   const T* rf;
   const T* gpm;  // finest level, precomputed Gauss-point moduli: K - 2G/3 at [g * n + e], G at [(8 + g) * n + e]
   RedTarget red;
-  double* err;   // tensor-core kernel: set to 1 when a bounded wait ran out
+  double* err;   // tensor-core kernel / TMA staging: set to 1 when a bounded wait ran out
+  alignas(64) CUtensorMap tmap;  // TMA staging: the staged vector as {px, ny, nz, 3} (finest applies)
 };
 using MechK = MechKT<double>;
 
@@ -189,8 +281,8 @@ __device__ __forceinline__ void mech_moduli_finest(const T (&Kn)[8], const T (&G
 // nodes: x-neighbours by one shuffle, y-neighbours through the register carry yp, z-neighbours
 // through the warp's shared-memory carry zc; then the epilogue of output node (x, ey, kk) when this
 // row step completes it.
-template <typename T, int EPI, int NF>
-__device__ __forceinline__ void assemble_row(const MechKT<T>& k, const Stream<NF, T>& st, int si, int lane, int x,
+template <typename T, int EPI, class ST>
+__device__ __forceinline__ void assemble_row(const MechKT<T>& k, const ST& st, int si, int lane, int x,
                                              int ey, int kk, int z0, int rr, const T (&f)[3][8], T (&yp)[2][3],
                                              T* zc, double& red0, double& red1, double& red2) {
   // ---- combine x-neighbours: node x gets own a=0 corners + left lane's a=1 corners
@@ -264,21 +356,40 @@ __device__ __forceinline__ void assemble_row(const MechKT<T>& k, const Stream<NF
 // T = double: the plain form; T = float: the precision form's V-cycle (reductions stay FP64).
 // GPM: the finest level's Gauss-point moduli come precomputed (gp_material_kernel) instead of being
 // interpolated from the staged nodal K, G, d in every apply.
-template <typename T, bool FINEST, int EPI, bool DIAG, bool ISO, bool GPM = false>
-__global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
+// TMA: the finest applies on precomputed moduli stage their rows with tensor copies (TmaStream)
+// instead of per-lane cp.async; the same values reach the same arithmetic, so the same bits.
+template <typename T, bool FINEST, int EPI, bool DIAG, bool ISO, bool GPM = false, bool TMA = false>
+__global__ void __launch_bounds__(kWarps * 32) mech_kernel(const __grid_constant__ MechKT<T> k) {
   constexpr int NU = DIAG ? 0 : 3;
   constexpr int NF = NU + (FINEST ? (GPM ? 0 : 3) : 2);
-  extern __shared__ __align__(16) unsigned char mech_smem[];
+  static_assert(!TMA || (FINEST && GPM && !DIAG), "TMA staging serves the finest applies on precomputed moduli");
+  extern __shared__ __align__(128) unsigned char mech_smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  // per warp: the staging ring, then the z-carry of the strip's wy - 1 output rows
-  T* ring = reinterpret_cast<T*>(mech_smem) + (size_t)wib * (kRing * NF * 2 * kRowW + (k.sg.wy - 1) * 3 * 32);
-  T* zc = ring + kRing * NF * 2 * kRowW;  // [row][comp][lane]
+  // per warp: [TMA: 4 mbarriers] the staging ring, then the z-carry of the strip's wy - 1 output rows
+  const size_t wbytes = TMA ? tma_warp_bytes<T>(k.sg.wy)
+                            : (size_t)(kRing * NF * 2 * kRowW + (k.sg.wy - 1) * 3 * 32) * sizeof(T);
+  // TMA: ring slots on 128-byte boundaries (the launch adds 128 bytes for this alignment)
+  unsigned char* base = TMA ? mech_smem + ((128u - (smem_u32(mech_smem) & 127u)) & 127u) : mech_smem;
+  unsigned char* wbase = base + (size_t)wib * wbytes;
+  T* ring = reinterpret_cast<T*>(wbase + (TMA ? kTmaHead : 0));
+  T* zc = ring + (TMA ? (size_t)kRing * TmaStream<T>::SLOT : (size_t)kRing * NF * 2 * kRowW);  // [row][comp][lane]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(wbase);
+  if constexpr (TMA) {
+    if (lane == 0) {
+#pragma unroll
+      for (int i = 0; i < kRing; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + i)) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncwarp();
+  }
   const SFt<T> s = make_sf<T>(k.g);
   double red0 = 0.0, red1 = 0.0, red2 = 0.0;
   const long long nwarps_total = (long long)gridDim.x * kWarps;
   const T* fptr[NF];
 #pragma unroll
   for (int f = 0; f < NF; ++f) fptr[f] = k.fields[f];
+  unsigned staged = 0;  // rows this warp staged so far (TMA: slot and barrier phase bookkeeping)
 
   for (long long strip = (long long)blockIdx.x * kWarps + wib; strip < k.sg.nstrips; strip += nwarps_total) {
     const int sx = (int)(strip % k.sg.tx);
@@ -289,92 +400,104 @@ __global__ void __launch_bounds__(kWarps * 32) mech_kernel(MechKT<T> k) {
     const int x0 = sx * kOX, y0 = sy * (wy - 1), z0 = sz * k.sg.cz;
     const int x = x0 - 1 + lane;
     const int zend = min(z0 + k.sg.cz - 1, k.g.nz - 1);
-    Stream<NF, T> st{ring, fptr, x, y0, z0, zend - z0 + 2, 0, rows, &k.g};
-    st.total = st.nlayers * rows;
-    st.issue(0, lane);
-    st.issue(1, lane);
-    T yp[2][3];
-    for (int si = 0; si < st.total; ++si) {
-      st.issue(si + 2, lane);
-      cp_async_wait2();
-      __syncwarp();
-      const int li = si / rows, r = si - li * rows;
-      const int kk = z0 - 1 + li;
-      if (r == 0) {
+    const int nlayers = zend - z0 + 2;
+    // one strip, whichever staging: rows issued two ahead, each row waited for before use
+    auto run_strip = [&](auto& st) -> bool {
+      st.issue(0, lane);
+      st.issue(1, lane);
+      T yp[2][3];
+      for (int si = 0; si < st.total; ++si) {
+        st.issue(si + 2, lane);
+        if (!st.wait(si)) return false;
+        const int li = si / rows, r = si - li * rows;
+        const int kk = z0 - 1 + li;
+        if (r == 0) {
 #pragma unroll
-        for (int c = 0; c < 2; ++c)
+          for (int c = 0; c < 2; ++c)
 #pragma unroll
-          for (int m = 0; m < 3; ++m) yp[c][m] = T(0);
+            for (int m = 0; m < 3; ++m) yp[c][m] = T(0);
+          __syncwarp();
+          continue;
+        }
+        const int rr = r - 1, ey = y0 - 1 + rr;
+        if (EPI == EPI_RESIDUAL && rr >= 1 && kk >= z0 && lane >= 1 && lane <= 30 && x < k.g.nx && ey < k.g.ny) {
+          // the epilogue reads f and M^-1 of this row's output node: start them towards L2 now, so
+          // their latency overlaps the element math instead of following it
+          const long long n = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(k.fu + n + m * k.g.n));
+            if (k.invM) asm volatile("prefetch.global.L2 [%0];" ::"l"(k.invM + n + m * k.g.n));
+          }
+        }
+        // ---- element (x, ey, kk) from stream rows si-1 (y = ey) and si (y = ey+1)
+        T f[3][8];
+        const bool valid = lane < 31 && x >= 0 && x <= k.g.nx - 2 && ey >= 0 && ey <= k.g.ny - 2 && kk >= 0 &&
+                           kk <= k.g.nz - 2;
+        if (valid) {
+          T Kw[8], Gw[8];
+          // ISO: the 1/h^2 of the two gradients goes into the Gauss weight (see sf_forward)
+          const T wg = ISO ? T(k.g.wg) * (s.ih[0] * s.ih[0]) : T(k.g.wg);
+          if (FINEST && GPM) {
+            const long long e = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+              Kw[g] = k.gpm[(long long)g * k.g.n + e];
+              Gw[g] = k.gpm[(long long)(8 + g) * k.g.n + e];
+            }
+          } else if (FINEST) {
+            T Kn[8], Gn[8], dn[8];
+#pragma unroll
+            for (int n = 0; n < 8; ++n) {
+              const int a = n & 1, b = (n >> 1) & 1, c = n >> 2;
+              const int srow = b ? si : si - 1;
+              Kn[n] = st.at(srow, NU + 0, c, lane + a);
+              Gn[n] = st.at(srow, NU + 1, c, lane + a);
+              dn[n] = st.at(srow, NU + 2, c, lane + a);
+            }
+            const long long e = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
+            mech_moduli_finest(Kn, Gn, dn, k.choice[e], T(k.small_k), wg, s, Kw, Gw);
+          } else {
+            const T K = st.at(si - 1, NU + 0, 0, lane) * wg, G = st.at(si - 1, NU + 1, 0, lane) * wg;
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+              Kw[g] = K;
+              Gw[g] = G;
+            }
+          }
+          if constexpr (DIAG) {
+            mech_element_diag(Kw, Gw, s, f);
+          } else {
+            T u[3][8];
+#pragma unroll
+            for (int n = 0; n < 8; ++n) {
+              const int a = n & 1, b = (n >> 1) & 1, c = n >> 2;
+              const int srow = b ? si : si - 1;
+#pragma unroll
+              for (int m = 0; m < 3; ++m) u[m][n] = st.at(srow, m, c, lane + a);
+            }
+            mech_element<ISO, T, FINEST && GPM>(u, Kw, Gw, s, f);
+          }
+        } else {
+#pragma unroll
+          for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int n = 0; n < 8; ++n) f[m][n] = T(0);
+        }
+        assemble_row<T, EPI>(k, st, si, lane, x, ey, kk, z0, rr, f, yp, zc, red0, red1, red2);
         __syncwarp();
-        continue;
       }
-      const int rr = r - 1, ey = y0 - 1 + rr;
-      if (EPI == EPI_RESIDUAL && rr >= 1 && kk >= z0 && lane >= 1 && lane <= 30 && x < k.g.nx && ey < k.g.ny) {
-        // the epilogue reads f and M^-1 of this row's output node: start them towards L2 now, so
-        // their latency overlaps the element math instead of following it
-        const long long n = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(k.fu + n + m * k.g.n));
-          if (k.invM) asm volatile("prefetch.global.L2 [%0];" ::"l"(k.invM + n + m * k.g.n));
-        }
-      }
-      // ---- element (x, ey, kk) from stream rows si-1 (y = ey) and si (y = ey+1)
-      T f[3][8];
-      const bool valid = lane < 31 && x >= 0 && x <= k.g.nx - 2 && ey >= 0 && ey <= k.g.ny - 2 && kk >= 0 &&
-                         kk <= k.g.nz - 2;
-      if (valid) {
-        T Kw[8], Gw[8];
-        // ISO: the 1/h^2 of the two gradients goes into the Gauss weight (see sf_forward)
-        const T wg = ISO ? T(k.g.wg) * (s.ih[0] * s.ih[0]) : T(k.g.wg);
-        if (FINEST && GPM) {
-          const long long e = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
-#pragma unroll
-          for (int g = 0; g < 8; ++g) {
-            Kw[g] = k.gpm[(long long)g * k.g.n + e];
-            Gw[g] = k.gpm[(long long)(8 + g) * k.g.n + e];
-          }
-        } else if (FINEST) {
-          T Kn[8], Gn[8], dn[8];
-#pragma unroll
-          for (int n = 0; n < 8; ++n) {
-            const int a = n & 1, b = (n >> 1) & 1, c = n >> 2;
-            const int srow = b ? si : si - 1;
-            Kn[n] = st.at(srow, NU + 0, c, lane + a);
-            Gn[n] = st.at(srow, NU + 1, c, lane + a);
-            dn[n] = st.at(srow, NU + 2, c, lane + a);
-          }
-          const long long e = (long long)x + (long long)ey * k.g.px + (long long)kk * k.g.plane;
-          mech_moduli_finest(Kn, Gn, dn, k.choice[e], T(k.small_k), wg, s, Kw, Gw);
-        } else {
-          const T K = st.at(si - 1, NU + 0, 0, lane) * wg, G = st.at(si - 1, NU + 1, 0, lane) * wg;
-#pragma unroll
-          for (int g = 0; g < 8; ++g) {
-            Kw[g] = K;
-            Gw[g] = G;
-          }
-        }
-        if constexpr (DIAG) {
-          mech_element_diag(Kw, Gw, s, f);
-        } else {
-          T u[3][8];
-#pragma unroll
-          for (int n = 0; n < 8; ++n) {
-            const int a = n & 1, b = (n >> 1) & 1, c = n >> 2;
-            const int srow = b ? si : si - 1;
-#pragma unroll
-            for (int m = 0; m < 3; ++m) u[m][n] = st.at(srow, m, c, lane + a);
-          }
-          mech_element<ISO, T, FINEST && GPM>(u, Kw, Gw, s, f);
-        }
-      } else {
-#pragma unroll
-        for (int m = 0; m < 3; ++m)
-#pragma unroll
-          for (int n = 0; n < 8; ++n) f[m][n] = T(0);
-      }
-      assemble_row<T, EPI, NF>(k, st, si, lane, x, ey, kk, z0, rr, f, yp, zc, red0, red1, red2);
-      __syncwarp();
+      return true;
+    };
+    if constexpr (TMA) {
+      constexpr int A = 16 / (int)sizeof(T);  // columns per 16 bytes: the copy's x start is a multiple
+      const int xs = x0 - 1 >= 0 ? (x0 - 1) / A * A : -A;
+      TmaStream<T> st{ring, bars, &k.tmap, xs, (x0 - 1) - xs, y0, z0, nlayers, nlayers * rows, rows, staged, k.err};
+      if (!run_strip(st)) break;
+      staged += (unsigned)st.total;
+    } else {
+      Stream<NF, T> st{ring, fptr, x, y0, z0, nlayers, nlayers * rows, rows, &k.g};
+      run_strip(st);
     }
   }
   if (EPI == EPI_RESIDUAL || EPI == EPI_PCG) {
@@ -696,7 +819,7 @@ __global__ void __launch_bounds__(kWarps * 32) mech_tc_kernel(MechKT<float> k) {
         for (int i = 0; i < 8; ++i) f[2][i] = a8[i];
       }
       tc_fence_before();
-      if (mine) assemble_row<T, EPI, NF>(k, st, si, lane, x, ey, kk, z0, rr, f, yp, zc, red0, red1, red2);
+      if (mine) assemble_row<T, EPI>(k, st, si, lane, x, ey, kk, z0, rr, f, yp, zc, red0, red1, red2);
       __syncwarp();
     }
   }
@@ -767,7 +890,9 @@ static int kernel_cfg(Kern kern, size_t max_smem, size_t smem, int* per_sm_out) 
       *per_sm_out = g_cfg[i].per_sm;
       return HPC_OK;
     }
-  if (max_smem > 48 * 1024) {
+  // opt in always: the 48 KB default bounds static plus dynamic shared memory together, and the
+  // kernels' own static share would push a dynamic size just below 48 KB over it
+  {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(smem)");
   }
@@ -905,11 +1030,53 @@ int tuned_shapes(int* out5, int cap) {
 // Isotropic spacing (hx = hy = hz) selects the kernels that fold 1/h^2 into the material.
 inline bool iso(const LevelGeo& g) { return g.hx == g.hy && g.hy == g.hz; }
 
+// The staged vector of a finest apply as a TMA tensor {px, ny, nz, 3} (x fastest; the three components
+// n apart), box {BX, 1, 2, 3}: one copy brings a row's three components on two planes.
+using EncodeTiled = PFN_cuTensorMapEncodeTiled_v12000;
+static EncodeTiled tensor_map_encoder() {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q{};
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  });
+  return fn;
+}
+template <typename T>
+static int encode_rows(const LevelGeo& g, const T* src, CUtensorMap* map) {
+  EncodeTiled enc = tensor_map_encoder();
+  if (!enc) {
+    set_error("TMA staging: cuTensorMapEncodeTiled unavailable");
+    return HPC_ERR_CUDA;
+  }
+  const cuuint64_t es = sizeof(T);
+  const cuuint64_t dims[4] = {(cuuint64_t)g.px, (cuuint64_t)g.ny, (cuuint64_t)g.nz, 3};
+  const cuuint64_t strides[3] = {(cuuint64_t)g.px * es, (cuuint64_t)g.plane * es, (cuuint64_t)g.n * es};
+  const cuuint32_t box[4] = {(cuuint32_t)TmaShape<T>::BX, 1, 2, 3};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = enc(map, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                         const_cast<T*>(src), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("TMA staging: cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return HPC_ERR_CUDA;
+  }
+  return HPC_OK;
+}
+
 template <bool F, int E, bool D, typename T = double>
-static int run_mech(hpc_ctx* c, const MechKT<T>& k) {
+static int run_mech(hpc_ctx* c, const MechKT<T>& k, bool tma = false) {
   const int cls = (F && E == EPI_PCG && !D) ? (sizeof(T) == 8 ? HPC_KC_MECH_PCG_FINEST : HPC_KC_MECH32_PCG_FINEST)
                                              : HPC_KC_NONE;
   if constexpr (F && !D) {
+    if (k.gpm && tma) {  // precomputed Gauss-point moduli, rows staged by tensor copies
+      const SmemPlan smem{128, (kTmaHead + (size_t)kRing * tma_slot_bytes<T>()) / sizeof(T), 3 * 32, sizeof(T)};
+      if (iso(k.g)) return launch_strips(c, mech_kernel<T, F, E, D, true, true, true>, k, smem, cls);
+      return launch_strips(c, mech_kernel<T, F, E, D, false, true, true>, k, smem, cls);
+    }
     if (k.gpm) {  // precomputed Gauss-point moduli: only u is staged
       constexpr int NF = 3;
       const SmemPlan smem{0, (size_t)kRing * NF * 2 * kRowW, 3 * 32, sizeof(T)};
@@ -956,15 +1123,21 @@ int launch_mech(hpc_ctx* c, const MechCall& m) {
   k.rf = m.rf;
   k.gpm = (m.finest && c->gpm_active) ? c->F[m.level].gpm : nullptr;
   k.red = make_red(c, m.s_out0, m.s_out1, m.s_out2);
+  k.err = c->scal + S_ERR;
   const bool f = m.finest;
+  const bool tma = f && k.gpm && c->tma_stage;
+  if (tma) {
+    const int rc = encode_rows<double>(k.g, k.fields[0], &k.tmap);
+    if (rc) return rc;
+  }
   switch (m.epi) {
-    case EPI_PLAIN: return f ? run_mech<true, EPI_PLAIN, false>(c, k) : run_mech<false, EPI_PLAIN, false>(c, k);
+    case EPI_PLAIN: return f ? run_mech<true, EPI_PLAIN, false>(c, k, tma) : run_mech<false, EPI_PLAIN, false>(c, k);
     case EPI_RESIDUAL:
-      return f ? run_mech<true, EPI_RESIDUAL, false>(c, k) : run_mech<false, EPI_RESIDUAL, false>(c, k);
-    case EPI_PCG: return f ? run_mech<true, EPI_PCG, false>(c, k) : run_mech<false, EPI_PCG, false>(c, k);
+      return f ? run_mech<true, EPI_RESIDUAL, false>(c, k, tma) : run_mech<false, EPI_RESIDUAL, false>(c, k);
+    case EPI_PCG: return f ? run_mech<true, EPI_PCG, false>(c, k, tma) : run_mech<false, EPI_PCG, false>(c, k);
     case EPI_FAS: return run_mech<false, EPI_FAS, false>(c, k);
     case EPI_REACTION:
-      return f ? run_mech<true, EPI_REACTION, false>(c, k) : run_mech<false, EPI_REACTION, false>(c, k);
+      return f ? run_mech<true, EPI_REACTION, false>(c, k, tma) : run_mech<false, EPI_REACTION, false>(c, k);
   }
   return HPC_ERR_ARG;
 }
@@ -1028,12 +1201,17 @@ int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
       case EPI_FAS: return run_mech_tc<false, EPI_FAS>(c, k);
     }
   }
+  const bool tma = fin && k.gpm && c->tma_stage;
+  if (tma) {
+    const int rc = encode_rows<float>(g, k.fields[0], &k.tmap);
+    if (rc) return rc;
+  }
   switch (m.epi) {
     case EPI_PLAIN:
-      return fin ? run_mech<true, EPI_PLAIN, false>(c, k) : run_mech<false, EPI_PLAIN, false>(c, k);
+      return fin ? run_mech<true, EPI_PLAIN, false>(c, k, tma) : run_mech<false, EPI_PLAIN, false>(c, k);
     case EPI_RESIDUAL:
-      return fin ? run_mech<true, EPI_RESIDUAL, false>(c, k) : run_mech<false, EPI_RESIDUAL, false>(c, k);
-    case EPI_PCG: return fin ? run_mech<true, EPI_PCG, false>(c, k) : run_mech<false, EPI_PCG, false>(c, k);
+      return fin ? run_mech<true, EPI_RESIDUAL, false>(c, k, tma) : run_mech<false, EPI_RESIDUAL, false>(c, k);
+    case EPI_PCG: return fin ? run_mech<true, EPI_PCG, false>(c, k, tma) : run_mech<false, EPI_PCG, false>(c, k);
     case EPI_FAS: return run_mech<false, EPI_FAS, false>(c, k);
   }
   return HPC_ERR_ARG;

@@ -379,7 +379,9 @@ static bool same_mg(const hpc_mg& a, const hpc_mg& b) {
 // parameters differ from the cached ones (the kernels' first use must already have happened,
 // `allow_capture`), replayed afterwards.  Kernel launches are counted per replay.  A graph is keyed
 // by its parameters and by `flags`, the context's kernel choices baked into its launches.
-static int graph_flags(const hpc_ctx* c) { return c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active; }
+static int graph_flags(const hpc_ctx* c) {
+  return c->tma_stage * 8 + c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active;
+}
 template <class Body>
 static int run_graphed(hpc_ctx* c, hpc_ctx::CoarseGraph& g, const hpc_mg& mg, double a, double b, bool allow_capture,
                        Body body, int flags) {
@@ -477,6 +479,19 @@ int gp_material(hpc_ctx* c, double small_k) {
   return HPC_OK;
 }
 
+// Kernels whose bounded waits ran out (tensor-core applies, TMA staging) report it in S_ERR.
+int check_wait_error(hpc_ctx* c) {
+  double err = 0.0;
+  int rc;
+  if ((rc = read_scalars(c, S_ERR, 1, &err))) return rc;
+  if (err != 0.0) {
+    write_scalar(c, S_ERR, 0.0);
+    set_error("a bounded wait in a kernel (tensor copy or MMA completion) ran out");
+    return HPC_ERR_CUDA;
+  }
+  return HPC_OK;
+}
+
 // u_entire (mechanical_displacement.cpp:25-115).
 static int u_entire_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, double mech_tol, int* cycles,
                         long long* fin_iters) {
@@ -522,6 +537,7 @@ static int u_entire_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut,
     }
     if (rel <= mech_tol) break;
   }
+  if (c->tma_stage && (rc = check_wait_error(c))) return rc;
   c->f_norm = f_norm;
   // externe_force_nodal (mechanical_right_hnd.cpp:18-38)
   if ((rc = launch_bc(c, L, c->F[L].u, nullptr, 0, Ut))) return rc;
@@ -832,15 +848,7 @@ static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double
     }
     rel = f_norm != 0 ? rn / f_norm : 1.0;
   }
-  if (mixed && c->tc_apply) {  // the tensor-core applies report a wait that ran out in S_ERR
-    double err = 0.0;
-    if ((rc = read_scalars(c, S_ERR, 1, &err))) return rc;
-    if (err != 0.0) {
-      write_scalar(c, S_ERR, 0.0);
-      set_error("tensor-core element apply: an MMA completion wait ran out");
-      return HPC_ERR_CUDA;
-    }
-  }
+  if (((mixed && c->tc_apply) || c->tma_stage) && (rc = check_wait_error(c))) return rc;
   c->f_norm = f_norm;
   // u = x, fu restored; externe_force_nodal (mechanical_right_hnd.cpp:18-38)
   HPC_CUDA(cudaMemcpyAsync(F.u, c->fcg.x, vbytes, cudaMemcpyDeviceToDevice, c->stream));
@@ -1139,6 +1147,12 @@ int hpc_set_tensor_apply(hpc_ctx* c, int on) {
 int hpc_set_fused_coarsest(hpc_ctx* c, int on) {
   if (!c) return arg_fail("null context");
   c->fused_coarsest = on != 0;
+  return HPC_OK;
+}
+
+int hpc_set_tma_staging(hpc_ctx* c, int on) {
+  if (!c) return arg_fail("null context");
+  c->tma_stage = on != 0;
   return HPC_OK;
 }
 
@@ -1577,8 +1591,13 @@ int step_end(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int p
 int step_end_finish(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int pcy, long long pit, double* out) {
   const double U_unit = 1.0;
   int rc;
-  double r3[3];
-  if ((rc = read_scalars(c, S_RES0, 3, r3))) return rc;
+  double r3[4];  // d maxima, top sum, and S_ERR: a bounded wait of a kernel in this increment ran out
+  if ((rc = read_scalars(c, S_RES0, 4, r3))) return rc;
+  if (r3[3] != 0.0) {
+    write_scalar(c, S_ERR, 0.0);
+    set_error("a bounded wait in a kernel (tensor copy or MMA completion) ran out");
+    return HPC_ERR_CUDA;
+  }
   const double FeW = r3[2] * p->voxel_size;
   const double Ut_now = c->Ut;
   c->Ut = c->Ut + c->dU;

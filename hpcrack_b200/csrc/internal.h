@@ -122,6 +122,7 @@ struct hpc_ctx {
   int tc_apply;        // precision form: element contraction on the tensor cores (hpc_set_tensor_apply)
   int fused_coarsest;  // coarse-level pcg_u in one block when the level fits (hpc_set_fused_coarsest)
   int gpm_active;      // finest applies read F[maxlevel].gpm (set while a mechanical solve runs)
+  int tma_stage;       // finest applies stage rows with tensor copies (hpc_set_tma_staging)
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
@@ -337,5 +338,6 @@ int step_end(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int p
 int step_end_enqueue(hpc_ctx* c);
 int step_end_finish(hpc_ctx* c, const hpc_step_params* p, int mcy, long long mit, int pcy, long long pit, double* out);
 int launch_set_scalar(hpc_ctx* c, int slot, double v);
+int check_wait_error(hpc_ctx* c);
 
 }  // namespace hpc

@@ -62,6 +62,7 @@ SIGNATURES = {
     "hpc_set_autotune": [_ctx, _i],
     "hpc_set_fused_coarsest": [_ctx, _i],
     "hpc_set_tensor_apply": [_ctx, _i],
+    "hpc_set_tma_staging": [_ctx, _i],
     "hpc_tuned_shapes": [_ip, _i, _ip],
     "hpc_launch_count": [_ctx, C.POINTER(C.c_longlong), _i],
     "hpc_binary_version": [_ip],

@@ -210,6 +210,10 @@ class Hierarchy:
         """Coarsest-level pcg_u in one thread block (default) or as per-iteration kernels."""
         self._c("hpc_set_fused_coarsest", int(bool(on)))
 
+    def set_tma_staging(self, on: bool = True):
+        """hpc_set_tma_staging: finest-level applies stage node rows with tensor copies (the same bits)."""
+        self._c("hpc_set_tma_staging", int(bool(on)))
+
     def set_autotune(self, on: bool):
         """Measure strip shapes on first use of each kernel and level size (see hpc_set_autotune)."""
         self._c("hpc_set_autotune", int(bool(on)))

@@ -139,6 +139,12 @@ int hpc_set_fused_coarsest(hpc_ctx* ctx, int on);
  * kernels.  TF32 operands approximate the FP32 operator to about 1e-3; the flexible PCG around the
  * V-cycle keeps its FP64 residual, so the solution meets the same tolerance. */
 int hpc_set_tensor_apply(hpc_ctx* ctx, int on);
+/* No counterpart in the reference: 1 stages the node rows of the finest-level operator applies
+ * (FP64 and the precision form's FP32, with the Gauss-point moduli of a mechanical solve) with
+ * tensor-memory-accelerator copies - one cp.async.bulk.tensor per row of three components on two
+ * planes, completion on an mbarrier - instead of per-lane cp.async; 0 (default) keeps cp.async.  The
+ * same values reach the same arithmetic: the same bits. */
+int hpc_set_tma_staging(hpc_ctx* ctx, int on);
 /* Kernels launched by this context since the last reset (instrumentation for benchmarks). */
 int hpc_launch_count(hpc_ctx* ctx, long long* count, int reset);
 /* The context's CUDA stream (cudaStream_t), for callers that time on it. */
