@@ -64,8 +64,9 @@ def parse_args():
     ap.add_argument("--mech-solver", choices=("fas", "fcg", "mixed"), default="fas",
                     help="fas: the reference's FAS V-cycles (plain form); fcg: flexible PCG preconditioned by one "
                          "FP64 V-cycle per iteration; mixed: the precision form (FP32 V-cycle, FP64 outer PCG)")
-    ap.add_argument("--tma", action="store_true",
-                    help="stage the finest applies' node rows with tensor copies (hpc_set_tma_staging)")
+    ap.add_argument("--no-tma", action="store_true",
+                    help="stage the finest applies' node rows with per-lane cp.async instead of tensor copies "
+                         "(hpc_set_tma_staging 0)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-timing", action="store_true")
@@ -151,7 +152,7 @@ def run_serving(args, local):
             q.workload.mg_u = v + (q.workload.mg_u[4],)
     kw = {"time_graphs": args.time_graphs} if args.engine == "batch" else {}
     server = sv.BatchServer if args.engine == "batch" else sv.SolveServer
-    srv = server(budget, args.slots, solver_factory=sv.default_factory(local),
+    srv = server(budget, args.slots, solver_factory=sv.default_factory(local, tma=not args.no_tma),
                  mech_solver=MECH_SOLVERS[args.mech_solver], precision_mg=not args.mg_u, **kw)
     from hpcrack_b200.solver import precision_mg
     mg_used = reqs[0].workload.mg_u
@@ -185,7 +186,7 @@ def batch_measure(local, n=64, increments=5, mech_solver="mixed", hbm_budget_gb=
     one CUDA graph per phase).  Returns solves/s, p50/p99 latency, wall time and the engine's timing."""
     from hpcrack_b200 import serving as sv
     reqs = [sv.Request(i, sv.batch_specimen(100 + i, increments), increments) for i in range(n)]
-    srv = sv.BatchServer(int(hbm_budget_gb * (1 << 30)), n, solver_factory=sv.default_factory(local),
+    srv = sv.BatchServer(int(hbm_budget_gb * (1 << 30)), n, solver_factory=sv.default_factory(local, tma=TMA_STAGING),
                          mech_solver=MECH_SOLVERS[mech_solver])
     t0 = time.perf_counter()
     res = srv.replay(reqs)
@@ -408,7 +409,7 @@ def workload_config(w, world, mech_solver="fas"):
 
 
 TENSOR_APPLY = False  # --tensor-apply
-TMA_STAGING = False   # --tma
+TMA_STAGING = True    # --no-tma turns it off
 
 
 def load_specimen(w, device):
@@ -417,8 +418,8 @@ def load_specimen(w, device):
     hier = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start, device=device)
     if TENSOR_APPLY:
         hier.set_tensor_apply(True)
-    if TMA_STAGING:
-        hier.set_tma_staging(True)
+    if not TMA_STAGING:
+        hier.set_tma_staging(False)
     hier.image_material(w.image, w.nodes, w.table(), w.voxel_size)
     if w.crack:
         Hc, dc = ms.precrack_fields(w)
@@ -504,7 +505,9 @@ def run_b200(args, rank, world, local):
         achieved = N * alg / (kms / kn / 1e3) / 1e9
         achieved_read = N * read / (kms / kn / 1e3) / 1e9
         peak, src = peaks()
-        kname = "mech_kernel<finest, PCG, Gauss-point moduli> (w = K(d) p, (p, w))"
+        kname = ("mech_kernel<finest, PCG, Gauss-point moduli, " +
+                 ("rows staged by TMA tensor copies" if TMA_STAGING else "rows staged by per-lane cp.async") +
+                 "> (w = K(d) p, (p, w))")
         basis = "algorithmic: u 24 + bulK,G,d 24 + regime 2 + out 24 B per finest node"
         roofline = {"bound": "hbm", "kernel": kname,
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -805,7 +808,7 @@ def main():
     global TENSOR_APPLY, TMA_STAGING
     args = parse_args()
     TENSOR_APPLY = args.tensor_apply
-    TMA_STAGING = args.tma
+    TMA_STAGING = not args.no_tma
     rank, world, local = dist_setup()
     try:
         if args.kernel_only:

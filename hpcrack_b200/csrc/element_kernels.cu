@@ -978,9 +978,9 @@ static int autotune_shape(hpc_ctx* c, Kern kern, Args a, const SmemPlan& plan, S
 }
 
 // Launches a strip kernel with the occupancy the device allows (persistent grid).  The strip shape
-// of the level comes from the latency model (choose_strips), or from a measurement when the context
-// has autotuning on (first use of a kernel on a level size, outside stream capture) or the process
-// measured it before.
+// of the level comes from the latency model (choose_strips), or - for a context with autotuning on -
+// from a measurement (first use of a kernel on a level size, outside stream capture, kept for every
+// autotuning context of the process).
 // `units`: the strip-shape model's parallel units (0: the SM sub-partitions).
 template <class Kern, class Args>
 static int launch_strips(hpc_ctx* c, Kern kern, Args a, const SmemPlan& plan, int cls, int ox = kOX,
@@ -989,9 +989,13 @@ static int launch_strips(hpc_ctx* c, Kern kern, Args a, const SmemPlan& plan, in
   if (units <= 0) units = (long long)num_sms() * 4;
   int dev = 0;
   cudaGetDevice(&dev);
-  if (!tuned_shape((const void*)kern, dev, a.g, &a.sg, ox)) {
+  // Measured shapes serve only contexts with autotuning on: a context without it always takes the
+  // model's shapes, so its results never depend on what another context measured.
+  if (!c->autotune) {
+    a.sg = choose_strips(a.g, units, ox);
+  } else if (!tuned_shape((const void*)kern, dev, a.g, &a.sg, ox)) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    if (c->autotune && cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+    if (cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
       if ((rc = autotune_shape(c, kern, a, plan, &a.sg, ox))) return rc;
       std::lock_guard<std::mutex> lock(g_tune_mu);
       if (g_ntuned < 512)

@@ -978,6 +978,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   c->use_graphs = 1;
   c->uid = ++g_ctx_uid;
   c->fused_coarsest = 1;
+  c->tma_stage = 1;  // tensor-copy staging of the finest applies: the same bits, 3 % faster on 257^3
   c->timing_class = HPC_KC_NONE;
   HostLevel lv[kMaxLevels];
   host_geometry(*geo, c->box, lv);

@@ -15,12 +15,12 @@ through a number of staggered increments (the loop of crack_propagation.cpp:65-1
 
 Each context's kernels are deterministic and contexts share no device state, so a request's result
 is the same bit for bit whether it runs alone or in a mix; ``tests/test_gpu_serving.py`` checks this.
-That holds with the strip shapes fixed in advance, as they are by default (the latency model).  With
-autotuning on (``hpc_set_autotune``) the first context to meet a level size measures the shapes under
-whatever load is running then and every later context reuses them; a different shape changes the
-summation order, so a request's bits can then differ between a run alone and a run in a mix (both
-still meet the same stopping test).  A server that wants autotuned shapes and bit-reproducible
-requests tunes every size once before admitting requests.
+That holds with the strip shapes of the latency model, as every context without autotuning has them.
+With autotuning on (``hpc_set_autotune``) the first autotuning context to meet a level size measures
+the shapes under whatever load is running then and every later autotuning context reuses them; a
+different shape changes the summation order, so such a request's bits can differ between a run alone
+and a run in a mix (both still meet the same stopping test).  A server that wants autotuned shapes and
+bit-reproducible requests tunes every size once before admitting requests.
 
 The solver is pluggable (``solver_factory``): the CUDA library's :class:`~hpcrack_b200.solver.Hierarchy`
 in production, any object with the same ``image_material`` / ``set`` / ``voigt_all_level`` /
@@ -63,11 +63,14 @@ class Result:
         return self.finished - self.arrival
 
 
-def default_factory(device: int = 0):
+def default_factory(device: int = 0, tma: bool = True):
     from .solver import Hierarchy
 
     def make(w: ms.Workload):
-        return Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start, device=device)
+        h = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start, device=device)
+        if not tma:
+            h.set_tma_staging(False)
+        return h
 
     return make
 
@@ -166,13 +169,19 @@ class SolveServer:
             th.join(timeout)
 
     def replay(self, requests: list[Request]):
-        """Submits `requests` at their arrival times (seconds after start) and waits for all."""
+        """Submits `requests` at their arrival times (seconds after start) and waits for all.  Requests
+        arriving at t = 0 are all queued before the server starts, so that a batch submitted at once
+        is admitted at once."""
+        ordered = sorted(requests, key=lambda r: r.arrival)
+        at_start = [r for r in ordered if r.arrival <= 0.0]
+        for req in at_start:
+            req.arrival = 0.0
+            self.submit(req)
         self.start()
-        for req in sorted(requests, key=lambda r: r.arrival):
+        for req in ordered[len(at_start):]:
             delay = req.arrival - self.now()
             if delay > 0:
                 time.sleep(delay)
-            req.arrival = max(req.arrival, 0.0)
             self.submit(req)
         self.close()
         if self.errors:

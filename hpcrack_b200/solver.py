@@ -211,7 +211,8 @@ class Hierarchy:
         self._c("hpc_set_fused_coarsest", int(bool(on)))
 
     def set_tma_staging(self, on: bool = True):
-        """hpc_set_tma_staging: finest-level applies stage node rows with tensor copies (the same bits)."""
+        """hpc_set_tma_staging: finest-level applies stage node rows with tensor copies (default) or
+        per-lane cp.async (False); the same bits either way."""
         self._c("hpc_set_tma_staging", int(bool(on)))
 
     def set_autotune(self, on: bool):

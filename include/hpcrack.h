@@ -142,8 +142,8 @@ int hpc_set_tensor_apply(hpc_ctx* ctx, int on);
 /* No counterpart in the reference: 1 stages the node rows of the finest-level operator applies
  * (FP64 and the precision form's FP32, with the Gauss-point moduli of a mechanical solve) with
  * tensor-memory-accelerator copies - one cp.async.bulk.tensor per row of three components on two
- * planes, completion on an mbarrier - instead of per-lane cp.async; 0 (default) keeps cp.async.  The
- * same values reach the same arithmetic: the same bits. */
+ * planes, completion on an mbarrier - instead of per-lane cp.async (the default); 0 stages with
+ * per-lane cp.async.  The same values reach the same arithmetic: the same bits. */
 int hpc_set_tma_staging(hpc_ctx* ctx, int on);
 /* Kernels launched by this context since the last reset (instrumentation for benchmarks). */
 int hpc_launch_count(hpc_ctx* ctx, long long* count, int reset);

@@ -147,3 +147,12 @@ def test_batch_server_admits_late_arrivals_between_rounds():
     assert len(res[0].outputs) == 6 and len(res[1].outputs) == 2
     assert 2 in FakeBatch.sizes  # the late request ran in the same calls as the first one
     assert res[1].admitted >= 0.03 - 1e-3
+
+
+def test_batch_submitted_at_once_runs_in_one_round_per_increment():
+    """Requests arriving at t = 0 are queued before the engine starts: every round holds all of them."""
+    FakeBatch.sizes = []
+    reqs = [_req(i, 9, arrival=0.0, increments=3) for i in range(12)]
+    srv = sv.BatchServer(hbm_budget=1000, slots=12, solver_factory=FakeSolver, batch_factory=FakeBatch)
+    srv.replay(reqs)
+    assert FakeBatch.sizes == [12, 12, 12]
