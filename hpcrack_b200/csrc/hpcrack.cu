@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -30,6 +31,52 @@ int cuda_fail(cudaError_t e, const char* where) {
 static int arg_fail(const std::string& msg) {
   g_err = msg;
   return HPC_ERR_ARG;
+}
+
+// ---------------------------------------------------------------- context memory
+// A context's device memory comes from the device's stream-ordered pool, allocated and released in
+// the order of the context's stream: releasing a finished request's memory does not synchronise the
+// whole device (cudaFree does) while other contexts run, and the pool keeps it for the next request
+// (release threshold raised once per device: the memory stays with the process).
+void pool_setup(int device) {
+  static std::mutex mu;
+  static bool done[64] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0 || device >= 64 || done[device]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done[device] = true;
+}
+cudaError_t ctx_alloc(hpc_ctx* c, void** p, size_t bytes) { return cudaMallocAsync(p, bytes, c->stream); }
+void ctx_free(hpc_ctx* c, void* p) {
+  if (p) cudaFreeAsync(p, c->stream);
+}
+
+// Pinned host slots for the contexts' scalar reads (64 doubles each), carved from chunks allocated
+// once per process: creating and destroying contexts allocates and frees no pinned memory (cudaFreeHost
+// synchronises the device).
+static std::mutex g_pin_mu;
+static std::vector<double*> g_pin_free;
+static double* pinned_slot() {
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  if (g_pin_free.empty()) {
+    constexpr int kSlots = 256;
+    double* chunk = nullptr;
+    if (cudaMallocHost((void**)&chunk, sizeof(double) * 64 * kSlots) != cudaSuccess) return nullptr;
+    for (int i = kSlots - 1; i >= 0; --i) g_pin_free.push_back(chunk + 64 * i);
+  }
+  double* p = g_pin_free.back();
+  g_pin_free.pop_back();
+  return p;
+}
+static void pinned_release(double* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  g_pin_free.push_back(p);
 }
 
 void timing_begin(hpc_ctx* c, int cls) {
@@ -470,7 +517,7 @@ int gp_material(hpc_ctx* c, double small_k) {
   LevelFields& F = c->F[c->maxlevel];
   if (!F.gpm) {
     const size_t bytes = sizeof(double) * 16 * (size_t)c->L[c->maxlevel].n;
-    HPC_CUDA(cudaMalloc((void**)&F.gpm, bytes));
+    HPC_CUDA(ctx_alloc(c, (void**)&F.gpm, bytes));
     HPC_CUDA(cudaMemsetAsync(F.gpm, 0, bytes, c->stream));  // non-element slots stay zero
   }
   int rc = launch_gp_material(c, small_k);
@@ -563,19 +610,19 @@ int ensure_f32(hpc_ctx* c) {
     LevelF32& F = c->F32[l];
     float** vec[] = {&F.u, &F.fu, &F.ru, &F.uold, &F.p, &F.w, &F.invM};
     for (float** p : vec) {
-      HPC_CUDA(cudaMalloc((void**)p, 3 * n * sizeof(float)));
+      HPC_CUDA(ctx_alloc(c, (void**)p, 3 * n * sizeof(float)));
       HPC_CUDA(cudaMemsetAsync(*p, 0, 3 * n * sizeof(float), c->stream));
     }
     float** mat_f[] = {&F.K, &F.G, &F.d};
     float** mat_c[] = {&F.Ke, &F.Ge};
     const bool fin = (l == c->maxlevel);
     if (fin && l > 0) {
-      HPC_CUDA(cudaMalloc((void**)&F.gpm, 16 * n * sizeof(float)));
+      HPC_CUDA(ctx_alloc(c, (void**)&F.gpm, 16 * n * sizeof(float)));
       HPC_CUDA(cudaMemsetAsync(F.gpm, 0, 16 * n * sizeof(float), c->stream));
     }
     for (int q = 0; q < (fin ? 3 : 2); ++q) {
       float** p = fin ? mat_f[q] : mat_c[q];
-      HPC_CUDA(cudaMalloc((void**)p, n * sizeof(float)));
+      HPC_CUDA(ctx_alloc(c, (void**)p, n * sizeof(float)));
       HPC_CUDA(cudaMemsetAsync(*p, 0, n * sizeof(float), c->stream));
     }
   }
@@ -690,7 +737,7 @@ int ensure_fcg(hpc_ctx* c) {
   const size_t bytes = sizeof(double) * 3 * (size_t)c->L[c->maxlevel].n;
   double** arrs[] = {&c->fcg.x, &c->fcg.r, &c->fcg.rp, &c->fcg.f, &c->fcg.p};
   for (double** a : arrs) {
-    HPC_CUDA(cudaMalloc((void**)a, bytes));
+    HPC_CUDA(ctx_alloc(c, (void**)a, bytes));
     HPC_CUDA(cudaMemsetAsync(*a, 0, bytes, c->stream));
   }
   return HPC_OK;
@@ -969,6 +1016,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   }
   if (device < 0 || device >= ndev) return arg_fail("bad device index");
   HPC_CUDA(cudaSetDevice(device));
+  pool_setup(device);
   hpc_ctx* c = new hpc_ctx();
   std::memset(c, 0, sizeof(*c));
   c->geo = *geo;
@@ -992,8 +1040,8 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   for (int l = 0; l <= c->maxlevel; ++l) flag_bytes += lv[l].nx + lv[l].ny + lv[l].nz;
   std::vector<uint8_t> hflags(flag_bytes);
   {
-    cudaError_t ae = cudaMalloc(&c->bc_dev_base, flag_bytes);
-    if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMalloc(flags)"));
+    cudaError_t ae = ctx_alloc(c, &c->bc_dev_base, flag_bytes);
+    if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMallocAsync(flags)"));
   }
   size_t off = 0;
   const double* B = c->box;
@@ -1031,7 +1079,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
     g.bz = dbase + h.nx + h.ny;
     off += h.nx + h.ny + h.nz;
   }
-  if (cudaMemcpy(c->bc_dev_base, hflags.data(), flag_bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+  if (cudaMemcpyAsync(c->bc_dev_base, hflags.data(), flag_bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError(), "flags upload"));
   // per-level arrays
   for (int l = 0; l <= c->maxlevel; ++l) {
@@ -1040,32 +1088,32 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
     double** scal[] = {&F.bulK, &F.G, &F.gc, &F.d, &F.H, &F.fd, &F.Ke, &F.Ge, &F.R, &F.dold, &F.preMd, &F.pd, &F.wd, &F.tmp1};
     double** vec[] = {&F.u, &F.fu, &F.ru, &F.uold, &F.preMu, &F.p, &F.w, &F.tmp3};
     for (double** p : scal) {
-      cudaError_t ae = cudaMalloc((void**)p, sizeof(double) * n);
-      if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMalloc(level field)"));
+      cudaError_t ae = ctx_alloc(c, (void**)p, sizeof(double) * n);
+      if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMallocAsync(level field)"));
       if (cudaMemsetAsync(*p, 0, sizeof(double) * n, c->stream) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "memset"));
     }
     for (double** p : vec) {
-      cudaError_t ae = cudaMalloc((void**)p, sizeof(double) * 3 * n);
-      if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMalloc(level vector)"));
+      cudaError_t ae = ctx_alloc(c, (void**)p, sizeof(double) * 3 * n);
+      if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMallocAsync(level vector)"));
       if (cudaMemsetAsync(*p, 0, sizeof(double) * 3 * n, c->stream) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "memset"));
     }
-    cudaError_t ae = cudaMalloc((void**)&F.choice, (size_t)n);
-    if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMalloc(choice)"));
+    cudaError_t ae = ctx_alloc(c, (void**)&F.choice, (size_t)n);
+    if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMallocAsync(choice)"));
     if (cudaMemsetAsync(F.choice, 0, (size_t)n, c->stream) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "memset"));
   }
   {
     const long long n = c->L[c->maxlevel].n;
-    cudaError_t ae = cudaMalloc((void**)&c->d_old, sizeof(double) * n);
-    if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMalloc(d_old)"));
+    cudaError_t ae = ctx_alloc(c, (void**)&c->d_old, sizeof(double) * n);
+    if (ae != cudaSuccess) return fail(cuda_fail(ae, "cudaMallocAsync(d_old)"));
     cudaMemsetAsync(c->d_old, 0, sizeof(double) * n, c->stream);
     c->partials_cap = 3 * 8192;
-    if ((ae = cudaMalloc((void**)&c->scal, sizeof(double) * kScalarPool)) != cudaSuccess) return fail(cuda_fail(ae, "scal"));
+    if ((ae = ctx_alloc(c, (void**)&c->scal, sizeof(double) * kScalarPool)) != cudaSuccess) return fail(cuda_fail(ae, "scal"));
     cudaMemsetAsync(c->scal, 0, sizeof(double) * kScalarPool, c->stream);
-    if ((ae = cudaMalloc((void**)&c->partials, sizeof(double) * c->partials_cap)) != cudaSuccess)
+    if ((ae = ctx_alloc(c, (void**)&c->partials, sizeof(double) * c->partials_cap)) != cudaSuccess)
       return fail(cuda_fail(ae, "partials"));
-    if ((ae = cudaMalloc((void**)&c->counter, sizeof(unsigned int) * 4)) != cudaSuccess) return fail(cuda_fail(ae, "counter"));
+    if ((ae = ctx_alloc(c, (void**)&c->counter, sizeof(unsigned int) * 4)) != cudaSuccess) return fail(cuda_fail(ae, "counter"));
     cudaMemsetAsync(c->counter, 0, sizeof(unsigned int) * 4, c->stream);
-    if ((ae = cudaMallocHost((void**)&c->hscal, sizeof(double) * 64)) != cudaSuccess) return fail(cuda_fail(ae, "pinned"));
+    if (!(c->hscal = pinned_slot())) return fail(cuda_fail(cudaErrorMemoryAllocation, "pinned"));
   }
   double N[64];
   shape_table(N);
@@ -1081,36 +1129,33 @@ int hpc_destroy(hpc_ctx* c) {
   if (!c) return HPC_OK;
   cudaSetDevice(c->device);
   vtk_release(c);
-  if (c->stream) cudaStreamSynchronize(c->stream);
   for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
     LevelFields& F = c->F[l];
     void* ptrs[] = {F.bulK, F.G, F.gc, F.d, F.H, F.fd, F.Ke, F.Ge, F.R, F.dold, F.preMd, F.pd, F.wd, F.tmp1,
                     F.u, F.fu, F.ru, F.uold, F.preMu, F.p, F.w, F.tmp3, F.choice, F.gpm};
-    for (void* p : ptrs)
-      if (p) cudaFree(p);
+    for (void* p : ptrs) ctx_free(c, p);
   }
-  if (c->d_old) cudaFree(c->d_old);
-  if (c->scal) cudaFree(c->scal);
-  if (c->partials) cudaFree(c->partials);
-  if (c->counter) cudaFree(c->counter);
-  if (c->bc_dev_base) cudaFree(c->bc_dev_base);
-  if (c->hscal) cudaFreeHost(c->hscal);
-  if (c->stage) cudaFree(c->stage);
-  for (int i = 0; i < 2 * c->tev_cap; ++i) cudaEventDestroy(c->tev[i]);
-  delete[] c->tev;
-  if (c->gmech.valid) cudaGraphExecDestroy(c->gmech.exec);
-  if (c->gpf.valid) cudaGraphExecDestroy(c->gpf.exec);
+  ctx_free(c, c->d_old);
+  ctx_free(c, c->scal);
+  ctx_free(c, c->partials);
+  ctx_free(c, c->counter);
+  ctx_free(c, c->bc_dev_base);
+  ctx_free(c, c->stage);
   {
     double* fa[] = {c->fcg.x, c->fcg.r, c->fcg.rp, c->fcg.f, c->fcg.p};
-    for (double* p : fa)
-      if (p) cudaFree(p);
+    for (double* p : fa) ctx_free(c, p);
   }
   for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
     LevelF32& G = c->F32[l];
     float* fa[] = {G.u, G.fu, G.ru, G.uold, G.p, G.w, G.invM, G.K, G.G, G.d, G.Ke, G.Ge, G.gpm};
-    for (float* p : fa)
-      if (p) cudaFree(p);
+    for (float* p : fa) ctx_free(c, p);
   }
+  if (c->stream) cudaStreamSynchronize(c->stream);  // every release in the pool before the stream goes
+  pinned_release(c->hscal);
+  for (int i = 0; i < 2 * c->tev_cap; ++i) cudaEventDestroy(c->tev[i]);
+  delete[] c->tev;
+  if (c->gmech.valid) cudaGraphExecDestroy(c->gmech.exec);
+  if (c->gpf.valid) cudaGraphExecDestroy(c->gpf.exec);
   if (c->g32.valid) cudaGraphExecDestroy(c->g32.exec);
   for (auto& gf : c->gfcg)
     if (gf.valid) cudaGraphExecDestroy(gf.exec);
@@ -1225,7 +1270,7 @@ int hpc_kernel_time(hpc_ctx* c, long long* launches, double* total_ms) {
 static int upload_dense(hpc_ctx* c, int level, double* d, const double* host) {
   if (!c->stage) {
     const LevelGeo& f = c->L[c->maxlevel];
-    HPC_CUDA(cudaMalloc((void**)&c->stage, sizeof(double) * (size_t)f.nx * f.ny * f.nz));
+    HPC_CUDA(ctx_alloc(c, (void**)&c->stage, sizeof(double) * (size_t)f.nx * f.ny * f.nz));
   }
   const LevelGeo& g = c->L[level];
   HPC_CUDA(cudaMemcpyAsync(c->stage, host, sizeof(double) * (size_t)g.nx * g.ny * g.nz, cudaMemcpyHostToDevice,
@@ -1803,11 +1848,11 @@ int hpc_image_material(hpc_ctx* c, const uint8_t* image, const int* voxel_n, int
   const size_t nvox = (size_t)voxel_n[0] * voxel_n[1] * voxel_n[2];
   uint8_t* dimg = nullptr;
   void* dtab = nullptr;
-  HPC_CUDA(cudaMalloc(&dimg, nvox));
+  HPC_CUDA(ctx_alloc(c, (void**)&dimg, nvox));
   const size_t tab_bytes = sizeof(int) * ngray + 3 * sizeof(double) * ngray + 64;
-  if (cudaMalloc(&dtab, tab_bytes) != cudaSuccess) {
-    cudaFree(dimg);
-    return cuda_fail(cudaErrorMemoryAllocation, "cudaMalloc(table)");
+  if (ctx_alloc(c, &dtab, tab_bytes) != cudaSuccess) {
+    ctx_free(c, dimg);
+    return cuda_fail(cudaErrorMemoryAllocation, "cudaMallocAsync(table)");
   }
   double* dE = (double*)dtab;
   double* dnu = dE + ngray;
@@ -1819,9 +1864,8 @@ int hpc_image_material(hpc_ctx* c, const uint8_t* image, const int* voxel_n, int
   cudaMemcpyAsync(dgc, gcv, sizeof(double) * ngray, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(dgray, gray, sizeof(int) * ngray, cudaMemcpyHostToDevice, c->stream);
   int rc = launch_image_material(c, dimg, voxel_n, ngray, dgray, dE, dnu, dgc, voxel_size);
-  cudaStreamSynchronize(c->stream);
-  cudaFree(dimg);
-  cudaFree(dtab);
+  ctx_free(c, dimg);
+  ctx_free(c, dtab);
   if (rc) return rc;
   for (int f : {HPC_BULK, HPC_G, HPC_GC})
     for (int l = c->maxlevel; l > 0; --l)
