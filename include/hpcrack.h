@@ -103,7 +103,12 @@ enum { HPC_MECH_FAS = 0, HPC_MECH_FCG = 1, HPC_MECH_MIXED = 2 };
 
 /* ---------------- context ---------------- */
 
-/* Allocates the device mirrors of the whole hierarchy on `device`. */
+/* Allocates the device mirrors of the whole hierarchy on `device` (initialize, initialization.cpp:
+ * 19-134, and the mg / mgvec containers of crack_propagation.cpp:40-45).  The memory comes from the
+ * device's default stream-ordered pool, in the order of the context's stream; the first context on a
+ * device raises that pool's release threshold, so memory a destroyed context returns stays with the
+ * process for the next context instead of going back to the driver (creating and destroying
+ * contexts while others run synchronises nothing). */
 int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device);
 int hpc_destroy(hpc_ctx* ctx);
 /* Device bytes a context of this geometry holds at most while it solves (admission by HBM
