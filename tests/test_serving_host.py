@@ -156,3 +156,20 @@ def test_batch_submitted_at_once_runs_in_one_round_per_increment():
     srv = sv.BatchServer(hbm_budget=1000, slots=12, solver_factory=FakeSolver, batch_factory=FakeBatch)
     srv.replay(reqs)
     assert FakeBatch.sizes == [12, 12, 12]
+
+
+def test_batch_server_reports_a_failed_round_and_releases_every_context():
+    """A batched call that fails (one context's error fails the whole hpc_batch_step) is reported for
+    the requests in that round; every context is closed and its memory released."""
+    class FailingBatch(FakeBatch):
+        def step(self, hiers, params):
+            if any(h.w.name == "r2" for h in hiers):
+                raise RuntimeError("batched step failed")
+            return super().step(hiers, params)
+
+    reqs = [_req(i, 9, arrival=0.0, increments=2) for i in range(4)]
+    srv = sv.BatchServer(hbm_budget=100, slots=4, solver_factory=FakeSolver, batch_factory=FailingBatch)
+    with pytest.raises(RuntimeError, match="failed"):
+        srv.replay(reqs)
+    assert FakeSolver.live == 0
+    assert srv._used == 0 and srv._active == 0
