@@ -574,6 +574,10 @@ int hpc_batch_step(hpc_batch* b, hpc_ctx* const* ctxs, int n, const hpc_step_par
       set_error("hpc_batch_step: every context must exist and live on the same device");
       return HPC_ERR_ARG;
     }
+    if (ctxs[i]->slab) {  // its exchanges and collectives cannot sit inside the batch's graphs
+      set_error("hpc_batch_step: a slab context steps through hpc_step");
+      return HPC_ERR_ARG;
+    }
     for (int j = 0; j < i; ++j)
       if (ctxs[j] == ctxs[i]) {
         set_error("hpc_batch_step: a context appears twice");

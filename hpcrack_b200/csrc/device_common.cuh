@@ -54,6 +54,9 @@ struct RedTarget {
   double* scal;          // scalar pool
   int slot[3];           // destination slots (-1 = discard)
 };
+// The reduction target of a context for the next launch; on a z-slab context the slots are also
+// recorded so that the launch check combines them over the ranks with `op` (a RedOp).
+RedTarget make_red(hpc_ctx* c, int s0, int s1, int s2, int op = RED_SUM);
 
 // Block-wide reduction of NR values per thread followed by a deterministic grid-wide
 // combination: every block stores its partials; the last block to finish combines them in
@@ -98,6 +101,10 @@ __device__ void grid_reduce(double (&v)[NR], const RedTarget& t) {
     if (lane == 0) *t.counter = 0u;
   }
 }
+
+// A z plane this rank owns: reductions sum over owned nodes only (realdomain, pcg_utilities.cpp:16-58);
+// every plane of a whole specimen.
+__device__ __forceinline__ bool owned_plane(const LevelGeo& g, int k) { return k >= g.oz0 && k < g.oz1; }
 
 // Dirichlet node sets of boundary_conditions.cpp:20-154 from the separable axis flags.
 struct BcFlags {

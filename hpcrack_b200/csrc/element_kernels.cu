@@ -314,6 +314,8 @@ __device__ __forceinline__ void assemble_row(const MechKT<T>& k, const ST& st, i
       } else if (EPI == EPI_RESIDUAL) {
         const BcFlags bc = bc_flags(k.g, x, ey, kk);
         const bool fix[3] = {bc.c0, bc.c1, bc.c2};
+        // a slab's ghost planes keep the sums as they are (a select: ghost values may be anything)
+        const bool own = owned_plane(k.g, kk);
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
           T fv = k.fu[n + m * N];
@@ -321,23 +323,37 @@ __device__ __forceinline__ void assemble_row(const MechKT<T>& k, const ST& st, i
             fv = tot[m];
             k.fu[n + m * N] = fv;
           }
-          if (k.red.slot[0] >= 0) red0 = fma((double)fv, (double)fv, red0);  // sums nobody reads are skipped
+          if (k.red.slot[0] >= 0) {  // sums nobody reads are skipped
+            const double s0 = fma((double)fv, (double)fv, red0);
+            red0 = own ? s0 : red0;
+          }
           const T rv = fix[m] ? T(0) : fv - tot[m];
           k.out[n + m * N] = rv;
-          if (k.invM) red1 = fma((double)rv, (double)(rv * k.invM[n + m * N]), red1);
-          if (k.red.slot[2] >= 0) red2 = fma((double)rv, (double)rv, red2);
+          if (k.invM) {
+            const double s1 = fma((double)rv, (double)(rv * k.invM[n + m * N]), red1);
+            red1 = own ? s1 : red1;
+          }
+          if (k.red.slot[2] >= 0) {
+            const double s2 = fma((double)rv, (double)rv, red2);
+            red2 = own ? s2 : red2;
+          }
         }
       } else if (EPI == EPI_PCG) {  // w = K p, (p, w)
+        const bool own = owned_plane(k.g, kk);
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
           k.out[n + m * N] = tot[m];
-          red0 = fma((double)st.at(si - 1, m, 0, lane), (double)tot[m], red0);
+          const double s0 = fma((double)st.at(si - 1, m, 0, lane), (double)tot[m], red0);
+          red0 = own ? s0 : red0;
         }
       } else if (EPI == EPI_FAS) {
-        // coarsen_f_standard_routine (multigrid_intergrid.cpp:124-342) fused with the coarse apply
+        // coarsen_f_standard_routine (multigrid_intergrid.cpp:124-342) fused with the coarse apply;
+        // a slab's lower ghost plane has no fine plane below it (its value comes from the neighbour)
+        const int fz = 2 * kk + k.g.zsh;
 #pragma unroll
         for (int m = 0; m < 3; ++m)
-          k.out[n + m * N] = tot[m] + full_weight(k.gf, k.rf + (long long)m * k.gf.n, 2 * x, 2 * ey, 2 * kk);
+          k.out[n + m * N] =
+              tot[m] + (fz >= 0 ? full_weight(k.gf, k.rf + (long long)m * k.gf.n, 2 * x, 2 * ey, fz) : T(0));
       } else if (EPI == EPI_REACTION) {
         // Dirichlet_force_u (boundary_conditions.cpp:69-111)
         const BcFlags bc = bc_flags(k.g, x, ey, kk);
@@ -846,7 +862,7 @@ static int num_sms() {
   return g_num_sms;
 }
 
-RedTarget make_red(hpc_ctx* c, int s0, int s1, int s2) {
+RedTarget make_red(hpc_ctx* c, int s0, int s1, int s2, int op) {
   RedTarget t;
   t.partials = c->partials;
   t.counter = c->counter;
@@ -854,6 +870,13 @@ RedTarget make_red(hpc_ctx* c, int s0, int s1, int s2) {
   t.slot[0] = s0;
   t.slot[1] = s1;
   t.slot[2] = s2;
+  if (c->slab) {
+    c->red_slot[0] = s0;
+    c->red_slot[1] = s1;
+    c->red_slot[2] = s2;
+    c->red_op = op;
+    c->red_pending = 1;
+  }
   return t;
 }
 
@@ -1114,6 +1137,9 @@ static void mech_fields(hpc_ctx* c, int level, bool finest, bool diag, const dou
 }
 
 int launch_mech(hpc_ctx* c, const MechCall& m) {
+  // the restriction reads the fine residual around each coarse node: a slab takes the neighbours'
+  // planes first (SendRecv(rf), multigrid_intergrid.cpp:393)
+  if (m.epi == EPI_FAS) HPC_SLAB_HALO(c, m.fine_level, m.rf, 3, sizeof(double));
   MechK k{};
   k.g = c->L[m.level];
   if (m.epi == EPI_FAS) k.gf = c->L[m.fine_level];
@@ -1370,14 +1396,21 @@ __global__ void __launch_bounds__(kWarps * 32) pf_kernel(PfK k) {
             const double fv = k.fd[n];
             const double rv = fv - tot;
             k.out[n] = rv;
-            red0 = fma(fv, fv, red0);
-            red1 = fma(rv, rv, red1);
-            if (k.invM) red2 = fma(rv, rv * k.invM[n], red2);
+            const bool own = owned_plane(k.g, kk);
+            const double s0 = fma(fv, fv, red0), s1 = fma(rv, rv, red1);
+            red0 = own ? s0 : red0;
+            red1 = own ? s1 : red1;
+            if (k.invM) {
+              const double s2 = fma(rv, rv * k.invM[n], red2);
+              red2 = own ? s2 : red2;
+            }
           } else if (EPI == EPI_PCG) {
             k.out[n] = tot;
-            red0 = fma(st.at(si - 1, 0, 0, lane), tot, red0);
+            const double s0 = fma(st.at(si - 1, 0, 0, lane), tot, red0);
+            red0 = owned_plane(k.g, kk) ? s0 : red0;
           } else if (EPI == EPI_FAS) {
-            k.out[n] = tot + full_weight(k.gf, k.rf, 2 * x, 2 * ey, 2 * kk);
+            const int fz = 2 * kk + k.g.zsh;
+            k.out[n] = tot + (fz >= 0 ? full_weight(k.gf, k.rf, 2 * x, 2 * ey, fz) : 0.0);
           }
         }
       }
@@ -1403,6 +1436,7 @@ static int run_pf(hpc_ctx* c, const PfK& k, bool finest) {
 }
 
 int launch_pf(hpc_ctx* c, const PfCall& p) {
+  if (p.epi == EPI_FAS) HPC_SLAB_HALO(c, p.fine_level, p.rf, 1, sizeof(double));  // SendRecv(rf), :356
   PfK k{};
   k.g = c->L[p.level];
   if (p.epi == EPI_FAS) k.gf = c->L[p.fine_level];

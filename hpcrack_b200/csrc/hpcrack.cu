@@ -835,6 +835,7 @@ int fcg_iteration(hpc_ctx* c, const hpc_mg& mg, double small_k, int k, bool mixe
 // iteration), *fin_iters = finest smoother iterations inside them.
 static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, double mech_tol,
                             int* cycles, long long* fin_iters, bool mixed) {
+  if (c->slab) return arg_fail("a slab runs the reference's FAS V-cycles (mech_solver HPC_MECH_FAS)");
   int rc;
   const int L = c->maxlevel;
   LevelFields& F = c->F[L];
@@ -1004,10 +1005,13 @@ int hpc_footprint(const hpc_geometry* geo, size_t* bytes) {
 
 static std::atomic<unsigned long long> g_ctx_uid{0};
 
-int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
+// hpc_create (a whole specimen) and hpc_create_slab (rank r of nr along z; `slab`).
+static int create_ctx(hpc_ctx** out, const hpc_geometry* geo, int device, int nr, int r, bool slab) {
   if (!out) return arg_fail("null output");
   *out = nullptr;
   if (!geometry_ok(geo)) return arg_fail("bad geometry");
+  SlabLevel sl[kMaxLevels];
+  if (!slab_levels(*geo, nr, r, sl)) return arg_fail("bad slab decomposition (every rank needs a coarsest plane)");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) {
@@ -1030,10 +1034,19 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   c->timing_class = HPC_KC_NONE;
   HostLevel lv[kMaxLevels];
   host_geometry(*geo, c->box, lv);
+  for (int l = 0; l <= c->maxlevel; ++l) lv[l].nz = sl[l].nz;  // this rank's planes (all of them for one rank)
   auto fail = [&](int rc) {
     hpc_destroy(c);
     return rc;
   };
+  if (slab) {
+    // every solve of a slab runs its per-iteration kernels: the one-block coarsest solve and the graphs
+    // of coarse parts would need the exchanges inside them
+    c->use_graphs = 0;
+    c->fused_coarsest = 0;
+    const int rc = slab_attach(c, nr, r);
+    if (rc) return fail(rc);
+  }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "stream"));
   // axis flags for the Dirichlet sets (boundary_conditions.cpp:20-68, coordinates as get_coordinate :14-18)
   size_t flag_bytes = 0;
@@ -1058,6 +1071,11 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
     g.hy = h.hy;
     g.hz = h.hz;
     g.wg = 0.125 * h.hx * h.hy * h.hz;
+    g.zb = sl[l].zb;
+    g.oz0 = sl[l].lo;
+    g.oz1 = sl[l].hi;
+    g.zsh = l < c->maxlevel ? 2 * sl[l].zb - sl[l + 1].zb : 0;
+    if (g.zsh != 0 && g.zsh != -1) return fail(arg_fail("slab levels do not nest"));
     uint8_t* fx = hflags.data() + off;
     uint8_t* fy = fx + h.nx;
     uint8_t* fz = fy + h.ny;
@@ -1070,7 +1088,7 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
       fy[j] = (uint8_t)((y == B[2] ? 1 : 0) | (y == 0.5 * (B[2] + B[3]) ? 2 : 0));
     }
     for (int k = 0; k < h.nz; ++k) {
-      const double z = B[4] + k * h.hz;
+      const double z = B[4] + (sl[l].zb + k) * h.hz;
       fz[k] = (uint8_t)((z == B[4] ? 1 : 0) | (z == B[5] ? 2 : 0));
     }
     uint8_t* dbase = (uint8_t*)c->bc_dev_base + off;
@@ -1125,10 +1143,20 @@ int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
   return HPC_OK;
 }
 
+int hpc_create(hpc_ctx** out, const hpc_geometry* geo, int device) {
+  return create_ctx(out, geo, device, 1, 0, false);
+}
+
+int hpc_create_slab(hpc_ctx** out, const hpc_geometry* geo, int device, int nranks, int rank) {
+  if (nranks < 1 || rank < 0 || rank >= nranks) return arg_fail("bad slab rank");
+  return create_ctx(out, geo, device, nranks, rank, true);
+}
+
 int hpc_destroy(hpc_ctx* c) {
   if (!c) return HPC_OK;
   cudaSetDevice(c->device);
   vtk_release(c);
+  slab_release(c);
   for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
     LevelFields& F = c->F[l];
     void* ptrs[] = {F.bulK, F.G, F.gc, F.d, F.H, F.fd, F.Ke, F.Ge, F.R, F.dold, F.preMd, F.pd, F.wd, F.tmp1,
@@ -1192,6 +1220,7 @@ int hpc_set_tensor_apply(hpc_ctx* c, int on) {
 
 int hpc_set_fused_coarsest(hpc_ctx* c, int on) {
   if (!c) return arg_fail("null context");
+  if (c->slab && on) return arg_fail("a slab solves its coarsest level with per-iteration kernels");
   c->fused_coarsest = on != 0;
   return HPC_OK;
 }
@@ -1204,6 +1233,8 @@ int hpc_set_tma_staging(hpc_ctx* c, int on) {
 
 int hpc_set_autotune(hpc_ctx* c, int on) {
   if (!c) return arg_fail("null context");
+  // trial launches differ between ranks, and every reducing launch of a slab is a collective step
+  if (c->slab && on) return arg_fail("no strip autotuning on a slab");
   c->autotune = on != 0;
   return HPC_OK;
 }
@@ -1769,7 +1800,7 @@ int hpc_initial_crack(hpc_ctx* c, double H_crack, int level) {
   for (int i = 0; i < g.nx; ++i) f[i] = (B[0] + i * g.hx) == B[1];
   for (int j = 0; j < g.ny; ++j) f[g.nx + j] = (B[2] + j * g.hy) == B[3];
   for (int k = 0; k < g.nz; ++k) {
-    const double z = B[4] + k * g.hz;
+    const double z = B[4] + (g.zb + k) * g.hz;
     f[g.nx + g.ny + k] = (z == 0.5 * (B[4] + B[5]) || z == 0.5 * (B[4] + B[5]) - gm.hz);
   }
   uint8_t* d = nullptr;
@@ -1839,7 +1870,7 @@ int hpc_image_material(hpc_ctx* c, const uint8_t* image, const int* voxel_n, int
   if (!c || !image || !voxel_n || ngray < 2 || !gray || !E || !nu || !gcv) return arg_fail("bad argument");
   const LevelGeo& g = c->L[c->maxlevel];
   for (int a = 0; a < 3; ++a) {
-    const int need = (a == 0 ? g.nx : a == 1 ? g.ny : g.nz) + c->geo.roi_start[a];
+    const int need = (a == 0 ? g.nx : a == 1 ? g.ny : g.zb + g.nz) + c->geo.roi_start[a];
     if (voxel_n[a] < need) {
       set_error("image smaller than the ROI of the finest grid");
       return HPC_ERR_INPUT;

@@ -30,6 +30,12 @@ struct LevelGeo {
   const uint8_t* bx;
   const uint8_t* by;
   const uint8_t* bz;
+  // z-slab decomposition (one specimen split along z over ranks, initialization.cpp:19-134): the
+  // global z index of local plane 0 (get_coordinate, boundary_conditions.cpp:13-18), the planes
+  // this rank owns [oz0, oz1) (realdomain.h:17-40; the others are ghost copies of a neighbour's
+  // planes), and on a coarse level the shift of its fine level: coarse plane kc sits on fine
+  // local plane 2 kc + zsh (0, or -1 on every rank but the first).  One rank: 0, [0, nz), 0.
+  int zb, oz0, oz1, zsh;
 };
 
 struct LevelFields {
@@ -123,6 +129,11 @@ struct hpc_ctx {
   int fused_coarsest;  // coarse-level pcg_u in one block when the level fits (hpc_set_fused_coarsest)
   int gpm_active;      // finest applies read F[maxlevel].gpm (set while a mechanical solve runs)
   int tma_stage;       // finest applies stage rows with tensor copies (hpc_set_tma_staging)
+  // z-slab rank of a specimen split over ranks (hpc_create_slab); null for a whole specimen.  A
+  // reduction launched on a slab context is combined over the ranks right after its launch
+  // (slab_after_launch): the launcher's make_red records its slots here.
+  struct SlabState* slab;
+  int red_slot[3], red_op, red_pending;
   // per-class launch timing (hpc_kernel_timing)
   int timing_class;
   cudaEvent_t* tev;  // 2 * tev_cap events: start/stop pairs
@@ -170,7 +181,34 @@ int cuda_fail(cudaError_t e, const char* where);
     (ctx)->launches++;                                                      \
     cudaError_t _e = cudaGetLastError();                                    \
     if (_e != cudaSuccess) return ::hpc::cuda_fail(_e, "kernel launch");    \
+    if ((ctx)->slab) {                                                      \
+      const int _r = ::hpc::slab_after_launch(ctx);                         \
+      if (_r) return _r;                                                    \
+    }                                                                       \
   } while (0)
+// Ghost planes of `ncomp` components (stride L[level].n elements of `elem` bytes) of a slab
+// context refreshed from the neighbouring ranks (SendRecv, mpi_communications.h:24-47, in z);
+// nothing for a whole specimen.
+#define HPC_SLAB_HALO(ctx, level, ptr, ncomp, elem)                         \
+  do {                                                                      \
+    if ((ctx)->slab) {                                                      \
+      const int _r = ::hpc::slab_halo(ctx, level, (void*)(ptr), ncomp, elem); \
+      if (_r) return _r;                                                    \
+    }                                                                       \
+  } while (0)
+
+// z-slab transport (slab.cu): the reduction recorded by make_red combined over the ranks (sum, max
+// or min in rank order, the same on every rank), and the ghost-plane exchange.
+int slab_after_launch(hpc_ctx* c);
+int slab_halo(hpc_ctx* c, int level, void* v, int ncomp, int elem_bytes);
+// Per-level z extents of rank r of nr (initialization.cpp:19-134, boundary_conditions.cpp:13-18,
+// realdomain.h:17-40): local planes, global index of local plane 0, owned planes [lo, hi).
+struct SlabLevel {
+  int nz, zb, lo, hi;
+};
+bool slab_levels(const hpc_geometry& g, int nr, int r, SlabLevel* out);
+int slab_attach(hpc_ctx* c, int nr, int r);  // a new context becomes rank r of nr
+void slab_release(hpc_ctx* c);
 
 // Launch timing: bracket a launch of class `cls` with events when that class is being timed.
 void timing_begin(hpc_ctx* c, int cls);

@@ -10,8 +10,6 @@
 
 namespace hpc {
 
-RedTarget make_red(hpc_ctx* c, int s0, int s1, int s2);
-
 namespace {
 
 int num_sms_v() {
@@ -57,7 +55,9 @@ template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
-template <typename T>
+// SLAB: sums over owned planes only (a z-slab context); the whole-specimen instance keeps the register
+// budget of the plain loop (48 against 58 with the test).
+template <typename T, bool SLAB = false>
 __global__ void mech_update_kernel(LevelGeo g, T* u, T* r, const T* p, const T* w, const T* invM, int s_rz, int s_pw,
                                    RedTarget red) {
   using V2 = typename Vec2<T>::type;
@@ -69,6 +69,7 @@ __global__ void mech_update_kernel(LevelGeo g, T* u, T* r, const T* p, const T* 
     const int i = 2 * (int)(q - row * half);
     const int kz = (int)(row / (unsigned)g.ny), j = (int)(row - (unsigned)kz * (unsigned)g.ny);
     const long long n = (long long)row * g.px + i;
+    const double rz0 = rz, rn0 = rn;
     bool fix[2][3] = {{false, false, false}, {false, false, false}};
     if (g.bz[kz]) {
 #pragma unroll
@@ -99,6 +100,10 @@ __global__ void mech_update_kernel(LevelGeo g, T* u, T* r, const T* p, const T* 
       rn = fma((double)rv.x, (double)rv.x, rn);
       rn = fma((double)rv.y, (double)rv.y, rn);
     }
+    if (SLAB && !owned_plane(g, kz)) {  // a ghost plane adds nothing (its values may be anything)
+      rz = rz0;
+      rn = rn0;
+    }
   }
   double v[3] = {rz, rn, 0.0};
   grid_reduce<3>(v, red);
@@ -111,8 +116,12 @@ int launch_mech_update_on(hpc_ctx* c, int level, double* x, double* r, const dou
   const int grid = (int)std::min<long long>((pairs + kRowThreads - 1) / kRowThreads, (long long)num_sms_v() * 8);
   const int cls = level == c->maxlevel ? HPC_KC_MECH_UPDATE_FINEST : HPC_KC_NONE;
   timing_begin(c, cls);
-  mech_update_kernel<<<grid, kRowThreads, 0, c->stream>>>(g, x, r, p, w, invM, s_num, s_den,
-                                                          make_red(c, s_rz_next, s_rn, -1));
+  if (c->slab)
+    mech_update_kernel<double, true><<<grid, kRowThreads, 0, c->stream>>>(g, x, r, p, w, invM, s_num, s_den,
+                                                                        make_red(c, s_rz_next, s_rn, -1));
+  else
+    mech_update_kernel<double, false><<<grid, kRowThreads, 0, c->stream>>>(g, x, r, p, w, invM, s_num, s_den,
+                                                                         make_red(c, s_rz_next, s_rn, -1));
   timing_end(c, cls);
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
@@ -132,6 +141,7 @@ template <typename TA>
 __global__ void dot2_kernel(LevelGeo g, const TA* a, const double* b, const double* cv, RedTarget red) {
   double s0 = 0.0, s1 = 0.0;
   FOR_NODES(g) {
+    if (!owned_plane(g, kz)) continue;
     const long long n = nidx(g, i, j, kz);
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
@@ -201,8 +211,10 @@ __global__ void pf_update_kernel(LevelGeo g, double* d, double* r, const double*
     d[n] = fma(p[n], alpha, d[n]);
     const double rv = fma(-w[n], alpha, r[n]);
     r[n] = rv;
-    rz = fma(rv, rv * invM[n], rz);
-    rn = fma(rv, rv, rn);
+    const bool own = owned_plane(g, kz);
+    const double z1 = fma(rv, rv * invM[n], rz), n1 = fma(rv, rv, rn);
+    rz = own ? z1 : rz;
+    rn = own ? n1 : rn;
   }
   double v[3] = {rz, rn, 0.0};
   grid_reduce<3>(v, red);
@@ -238,6 +250,7 @@ int launch_dir_update(hpc_ctx* c, int level, int ncomp, const double* r, const d
   dir_update_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, ncomp, r, invM, p, first ? 1 : 0, c->scal, s_rz,
                                                                s_rz_prev);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, level, p, ncomp, sizeof(double));  // SendRecv(z), mechanical_pcg.cpp:278, phase_field_pcg.cpp:180
   return HPC_OK;
 }
 
@@ -279,6 +292,7 @@ int launch_bc(hpc_ctx* c, int level, double* v, const double* src, int kind, dou
 __global__ void dot_kernel(LevelGeo g, int ncomp, const double* a, const double* b, RedTarget red) {
   double s = 0.0;
   FOR_NODES(g) {
+    if (!owned_plane(g, kz)) continue;
     const long long n = nidx(g, i, j, kz);
     for (int m = 0; m < ncomp; ++m) {
       const long long o = n + (long long)m * g.n;
@@ -348,15 +362,20 @@ int launch_axpby(hpc_ctx* c, double* y, const double* a, const double* b, double
 // inter-grid transfers (multigrid_intergrid.cpp)
 // ---------------------------------------------------------------------------------------------
 // solution_injection (:25-90)
+// On a z slab, coarse plane kc lies on fine plane 2 kc + zsh; a lower ghost plane without a fine
+// plane below it is left to the ghost exchange that follows every transfer.
 __global__ void inject_kernel(LevelGeo gc, LevelGeo gf, const double* f, double* co, int ncomp) {
   FOR_NODES(gc) {
-    const long long nc = nidx(gc, i, j, kz), nf = nidx(gf, 2 * i, 2 * j, 2 * kz);
+    const int fz = 2 * kz + gc.zsh;
+    if (fz < 0) continue;
+    const long long nc = nidx(gc, i, j, kz), nf = nidx(gf, 2 * i, 2 * j, fz);
     for (int m = 0; m < ncomp; ++m) co[nc + m * gc.n] = f[nf + m * gf.n];
   }
 }
 int launch_inject(hpc_ctx* c, int lf, const double* f, double* co, int ncomp) {
   inject_kernel<<<row_grid(c->L[lf - 1]), kRowThreads, 0, c->stream>>>(c->L[lf - 1], c->L[lf], f, co, ncomp);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, lf - 1, co, ncomp, sizeof(double));
   return HPC_OK;
 }
 
@@ -364,7 +383,9 @@ int launch_inject(hpc_ctx* c, int lf, const double* f, double* co, int ncomp) {
 template <typename T>
 __global__ void inject_u_kernel(LevelGeo gc, LevelGeo gf, const T* uf, T* uc, T* uold, T Ut) {
   FOR_NODES(gc) {
-    const long long nc = nidx(gc, i, j, kz), nf = nidx(gf, 2 * i, 2 * j, 2 * kz);
+    const int fz = 2 * kz + gc.zsh;
+    if (fz < 0) continue;
+    const long long nc = nidx(gc, i, j, kz), nf = nidx(gf, 2 * i, 2 * j, fz);
     T v[3] = {uf[nf], uf[nf + gf.n], uf[nf + 2 * gf.n]};
     if (gc.bz[kz]) {
       const BcFlags bc = bc_flags(gc, i, j, kz);
@@ -383,13 +404,17 @@ int launch_inject_u(hpc_ctx* c, int lf, double Ut) {
   inject_u_kernel<<<row_grid(c->L[lf - 1]), kRowThreads, 0, c->stream>>>(
       c->L[lf - 1], c->L[lf], c->F[lf].u, c->F[lf - 1].u, c->F[lf - 1].uold, Ut);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, lf - 1, c->F[lf - 1].u, 3, sizeof(double));  // SendRecv(uc), multigrid_intergrid.cpp:116
+  HPC_SLAB_HALO(c, lf - 1, c->F[lf - 1].uold, 3, sizeof(double));
   return HPC_OK;
 }
 
 // coarsen_d (:92-103)
 __global__ void inject_d_kernel(LevelGeo gc, LevelGeo gf, const double* df, double* dc, double* dold) {
   FOR_NODES(gc) {
-    const long long nc = nidx(gc, i, j, kz), nf = nidx(gf, 2 * i, 2 * j, 2 * kz);
+    const int fz = 2 * kz + gc.zsh;
+    if (fz < 0) continue;
+    const long long nc = nidx(gc, i, j, kz), nf = nidx(gf, 2 * i, 2 * j, fz);
     const double v = df[nf];
     dc[nc] = v;
     dold[nc] = v;
@@ -399,6 +424,8 @@ int launch_inject_d(hpc_ctx* c, int lf) {
   inject_d_kernel<<<row_grid(c->L[lf - 1]), kRowThreads, 0, c->stream>>>(c->L[lf - 1], c->L[lf], c->F[lf].d,
                                                                           c->F[lf - 1].d, c->F[lf - 1].dold);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, lf - 1, c->F[lf - 1].d, 1, sizeof(double));  // SendRecv(dc), multigrid_intergrid.cpp:99
+  HPC_SLAB_HALO(c, lf - 1, c->F[lf - 1].dold, 1, sizeof(double));
   return HPC_OK;
 }
 
@@ -406,13 +433,18 @@ int launch_inject_d(hpc_ctx* c, int lf) {
 __global__ void restrict_kernel(LevelGeo gc, LevelGeo gf, const double* rf, const double* Fic, double* fc, int ncomp) {
   FOR_NODES(gc) {
     const long long nc = nidx(gc, i, j, kz);
+    const int fz = 2 * kz + gc.zsh;
     for (int m = 0; m < ncomp; ++m)
-      fc[nc + m * gc.n] = Fic[nc + m * gc.n] + full_weight(gf, rf + m * gf.n, 2 * i, 2 * j, 2 * kz);
+      fc[nc + m * gc.n] = Fic[nc + m * gc.n] + (fz >= 0 ? full_weight(gf, rf + m * gf.n, 2 * i, 2 * j, fz) : 0.0);
   }
 }
 int launch_restrict(hpc_ctx* c, int lf, const double* rf, const double* Fic, double* fc, int ncomp) {
+  HPC_SLAB_HALO(c, lf, rf, ncomp, sizeof(double));  // SendRecv(rf), multigrid_intergrid.cpp:356,393
   restrict_kernel<<<row_grid(c->L[lf - 1]), kRowThreads, 0, c->stream>>>(c->L[lf - 1], c->L[lf], rf, Fic, fc, ncomp);
   HPC_CHECK_LAUNCH(c);
+  // SendRecv(fc), :369,411.  (The solves' fused restriction skips it: there the coarse right-hand side
+  // on ghost planes only feeds ghost residuals, which the next restriction takes from the neighbours.)
+  HPC_SLAB_HALO(c, lf - 1, fc, ncomp, sizeof(double));
   return HPC_OK;
 }
 
@@ -422,8 +454,9 @@ template <typename T>
 __global__ void prolong_kernel(LevelGeo gc, LevelGeo gf, const T* uc, const T* ucold, T* uf, int ncomp, int apply_bc,
                                T Ut) {
   FOR_NODES(gf) {
-    const int ox = i & 1, oy = j & 1, oz = kz & 1;
-    const int ic = (i + 1) >> 1, jc = (j + 1) >> 1, kc = (kz + 1) >> 1;
+    const int zq = kz - gc.zsh;  // fine plane counted from the coarse grid's plane 0
+    const int ox = i & 1, oy = j & 1, oz = zq & 1;
+    const int ic = (i + 1) >> 1, jc = (j + 1) >> 1, kc = (zq + 1) >> 1;
     const long long nf = nidx(gf, i, j, kz);
     BcFlags bc{false, false, false, false};
     if (apply_bc && gf.bz[kz]) bc = bc_flags(gf, i, j, kz);
@@ -463,6 +496,7 @@ int launch_prolong(hpc_ctx* c, int lf, const double* uc, const double* ucold, do
   prolong_kernel<<<row_grid(c->L[lf]), kRowThreads, 0, c->stream>>>(c->L[lf - 1], c->L[lf], uc, ucold, uf, ncomp,
                                                                      apply_bc ? 1 : 0, Ut);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, lf, uf, ncomp, sizeof(double));  // SendRecv(uf), multigrid_intergrid.cpp:531,547
   return HPC_OK;
 }
 
@@ -476,6 +510,7 @@ struct ChoiceK {
   double *Ke, *Ge;
   double small_k;
   int quirk, do_choice, do_element;
+  int nzg;  // planes of the whole specimen on this level (a slab evaluates the quirk on global planes)
 };
 
 __device__ __forceinline__ void load8(const double* f, const LevelGeo& g, int i, int j, int k, double (&v)[8]) {
@@ -496,12 +531,13 @@ __global__ void choice_kernel(ChoiceK a) {
       load8(a.G, g, i, j, k, Gn);
       gp_material(Kn, s, Kg);
       gp_material(Gn, s, Gg);
-      // the reference's loop bounds use the dense extent nx; the flat slot is i + j*nx + k*nx*ny
-      const long long flat = (long long)i + (long long)j * g.nx + (long long)k * g.nx * g.ny;
+      // the reference's loop bounds use the dense extent nx; the flat slot is i + j*nx + k*nx*ny, on the
+      // whole specimen's planes, so that a z-split regime field equals the unsplit one
+      const long long flat = (long long)i + (long long)j * g.nx + (long long)(g.zb + k) * g.nx * g.ny;
       int ch = 0;
       if (!a.do_choice) {
         ch = a.choice[e];
-      } else if (!a.quirk || choice_in_image(flat, g.nx, g.ny, g.nz)) {
+      } else if (!a.quirk || choice_in_image(flat, g.nx, g.ny, a.nzg)) {
         double gx[3][4], gy[3][4], gz[3][4];
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
@@ -547,7 +583,7 @@ int launch_choice_level(hpc_ctx* c, int level, double small_k, bool do_choice, b
   if (do_choice) HPC_CUDA(cudaMemsetAsync(F.choice, 0, (size_t)g.n, c->stream));
   if (g.nx < 2 || g.ny < 2 || g.nz < 2) return HPC_OK;
   ChoiceK a{g, F.u, F.bulK, F.G, F.d, F.choice, F.Ke, F.Ge, small_k, c->choice_quirk, do_choice ? 1 : 0,
-            do_element ? 1 : 0};
+            do_element ? 1 : 0, c->geo.element_nb[2] * (1 << level) + 1};
   long long rows = (long long)(g.ny - 1) * (g.nz - 1);
   int grid = (int)(rows < num_sms_v() * 8LL ? rows : num_sms_v() * 8LL);
   choice_kernel<<<grid, 128, 0, c->stream>>>(a);
@@ -571,7 +607,8 @@ __global__ void vr_kernel(LevelGeo gc, LevelGeo gf, const double* Hf, double* Hc
       if (whole) Hc[nc] = 0.0;
       continue;
     }
-    const int x = 2 * i, y = 2 * j, z = 2 * kz;
+    const int x = 2 * i, y = 2 * j, z = 2 * kz + gc.zsh;
+    if (z < 0) continue;
     const double h[8] = {Hf[nidx(gf, x, y, z)],         Hf[nidx(gf, x + 1, y, z)],
                          Hf[nidx(gf, x, y + 1, z)],     Hf[nidx(gf, x + 1, y + 1, z)],
                          Hf[nidx(gf, x, y, z + 1)],     Hf[nidx(gf, x + 1, y, z + 1)],
@@ -589,13 +626,15 @@ int launch_vr(hpc_ctx* c, int lf, const double* Hf, double* Hc, bool hill, bool 
   vr_kernel<<<row_grid(c->L[lf - 1]), kRowThreads, 0, c->stream>>>(c->L[lf - 1], c->L[lf], Hf, Hc, hill ? 1 : 0,
                                                                     whole_array ? 1 : 0);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, lf - 1, Hc, 1, sizeof(double));  // SendRecv(H), material_coarse_element.cpp:98,114
   return HPC_OK;
 }
 
 // voight / reuss / coarse_VR (image_input.cpp:144-260): 27-point clamped means, Hill combination.
 __global__ void coarse_vr_kernel(LevelGeo gc, LevelGeo gf, const double* f, double* co) {
   FOR_NODES(gc) {
-    const int x = 2 * i, y = 2 * j, z = 2 * kz;
+    const int x = 2 * i, y = 2 * j, z = 2 * kz + gc.zsh;
+    if (z < 0) continue;
     const int Xl = gf.nx - 1, Yl = gf.ny - 1, Zl = gf.nz - 1;
     const int xm = max(x - 1, 0), xp = min(x + 1, Xl), ym = max(y - 1, 0), yp = min(y + 1, Yl);
     const int zm = max(z - 1, 0), zp = min(z + 1, Zl);
@@ -617,6 +656,7 @@ __global__ void coarse_vr_kernel(LevelGeo gc, LevelGeo gf, const double* f, doub
 int launch_coarse_vr(hpc_ctx* c, int lf, const double* f, double* co) {
   coarse_vr_kernel<<<row_grid(c->L[lf - 1]), kRowThreads, 0, c->stream>>>(c->L[lf - 1], c->L[lf], f, co);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, lf - 1, co, 1, sizeof(double));  // SendRecv(MP), image_input.cpp:269
   return HPC_OK;
 }
 
@@ -714,8 +754,10 @@ __global__ void dmax_kernel(LevelGeo g, const double* d, double* dold, int copy,
   FOR_NODES(g) {
     const long long n = nidx(g, i, j, kz);
     const double v = d[n];
-    dd = fmax(dd, v - dold[n]);
-    dm = fmax(dm, v);
+    if (owned_plane(g, kz)) {
+      dd = fmax(dd, v - dold[n]);
+      dm = fmax(dm, v);
+    }
     if (copy) dold[n] = v;
   }
   double r[2] = {dd, dm};
@@ -725,7 +767,7 @@ int launch_dmax(hpc_ctx* c, int slot_dd, int slot_dmax, bool copy_old) {
   const int L = c->maxlevel;
   const LevelGeo& g = c->L[L];
   dmax_kernel<<<row_grid(g), kRowThreads, 0, c->stream>>>(g, c->F[L].d, c->d_old, copy_old ? 1 : 0,
-                                                         make_red(c, slot_dd, slot_dmax, -1));
+                                                         make_red(c, slot_dd, slot_dmax, -1, RED_MAX));
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
 }
@@ -780,7 +822,7 @@ int launch_ue(hpc_ctx* c, double lc, int slot) {
   long long rows = (long long)(g.ny - 1) * (g.nz - 1);
   int grid = (int)(rows < num_sms_v() * 8LL ? rows : num_sms_v() * 8LL);
   if (grid <= 0) grid = 1;
-  ue_kernel<<<grid, 128, 0, c->stream>>>(g, F.u, F.bulK, F.G, F.gc, lc, make_red(c, slot, -1, -1));
+  ue_kernel<<<grid, 128, 0, c->stream>>>(g, F.u, F.bulK, F.G, F.gc, lc, make_red(c, slot, -1, -1, RED_MIN));
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
 }
@@ -788,9 +830,10 @@ int launch_ue(hpc_ctx* c, double lc, int slot) {
 // externe_force_sum (mechanical_right_hnd.cpp:40-59): sum of fu_z over the top node plane.
 __global__ void top_sum_kernel(LevelGeo g, const double* fz, RedTarget red) {
   double s = 0.0;
-  const int k = g.nz - 1;
-  for (long long j = blockIdx.x; j < g.ny; j += gridDim.x)
-    for (int i = threadIdx.x; i < g.nx; i += blockDim.x) s += fz[nidx(g, i, (int)j, k)];
+  const int k = g.nz - 1;  // a slab rank below the top holds a ghost copy there: it adds nothing
+  if (owned_plane(g, k))
+    for (long long j = blockIdx.x; j < g.ny; j += gridDim.x)
+      for (int i = threadIdx.x; i < g.nx; i += blockDim.x) s += fz[nidx(g, i, (int)j, k)];
   double r[1] = {s};
   grid_reduce<1>(r, red);
 }
@@ -825,7 +868,7 @@ __global__ void image_material_kernel(LevelGeo g, const uint8_t* img, int vnx, i
                                       const double* gcv, double voxel, double* bulK, double* G, double* gc,
                                       int* err) {
   FOR_NODES(g) {
-    const long long vx = (long long)rx + i + (long long)vnx * (ry + j) + (long long)vnx * vny * (rz + kz);
+    const long long vx = (long long)rx + i + (long long)vnx * (ry + j) + (long long)vnx * vny * (rz + g.zb + kz);
     const int gl = img[vx];
     int p = -1;
     for (int q = 0; q < ngray - 1; ++q)
@@ -870,6 +913,7 @@ int launch_image_material(hpc_ctx* c, const uint8_t* dimage, const int* voxel_n,
 __global__ void zero_count_kernel(LevelGeo g, int ncomp, const double* v, RedTarget red) {
   double cnt = 0.0;
   FOR_NODES(g) {
+    if (!owned_plane(g, kz)) continue;
     const long long n = nidx(g, i, j, kz);
     for (int m = 0; m < ncomp; ++m) cnt += (v[n + m * g.n] == 0.0) ? 1.0 : 0.0;
   }

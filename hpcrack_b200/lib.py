@@ -119,6 +119,14 @@ SIGNATURES = {
     "hpc_refine_standard": [_ctx, _i, _i, _i, _i, _i],
     "hpc_image_material": [_ctx, C.POINTER(C.c_uint8), _ip, _i, _ip, _dp, _dp, _dp, _d],
     "hpc_dmax_noalloc": [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p],
+    "hpc_slab_level": [C.POINTER(hpc_geometry), _i, _i, _i, _ip],
+    "hpc_create_slab": [C.POINTER(C.c_void_p), C.POINTER(hpc_geometry), _i, _i, _i],
+    "hpc_slab_group_create": [C.POINTER(C.c_void_p), _i],
+    "hpc_slab_group_join": [_vp, _ctx],
+    "hpc_slab_group_abort": [_vp],
+    "hpc_slab_group_destroy": [_vp],
+    "hpc_nccl_unique_id": [C.POINTER(C.c_ubyte)],
+    "hpc_slab_join_nccl": [_ctx, C.POINTER(C.c_ubyte)],
 }
 _RESTYPE = {"hpc_last_error": C.c_char_p, "hpc_stream": C.c_void_p}
 

@@ -114,19 +114,42 @@ class Batch:
         self.close()
 
 
+def slab_level(maxlevel, enb, nranks, rank, level):
+    """(local nz, global z of local plane 0, first owned plane, one past the last) of a z-slab rank on
+    `level` (hpc_slab_level; host only)."""
+    lib = _L.load()
+    geo = _L.hpc_geometry(int(maxlevel), (C.c_int * 3)(*map(int, enb)), (C.c_double * 3)(0.0, 0.0, 0.0),
+                          (C.c_int * 3)(0, 0, 0))
+    out = (C.c_int * 4)()
+    _L.check("hpc_slab_level", lib.hpc_slab_level(C.byref(geo), int(nranks), int(rank), int(level), out))
+    return tuple(out)
+
+
 class Hierarchy:
     """Device-resident multigrid hierarchy of one specimen."""
 
-    def __init__(self, maxlevel, enb, x0=(0.0, 0.0, 0.0), roi=(0, 0, 0), device: int = 0):
+    def __init__(self, maxlevel, enb, x0=(0.0, 0.0, 0.0), roi=(0, 0, 0), device: int = 0, slab=None):
+        """slab = (nranks, rank): this context holds rank `rank`'s z planes of a specimen split over
+        `nranks` ranks (hpc_create_slab); its arrays (dims, set, get) are the local ones, ghost planes
+        included, and it joins a transport (hpcrack_b200.slab) before it solves."""
         self.lib = _L.load()
         self.maxlevel = int(maxlevel)
         self.enb = tuple(int(e) for e in enb)
         self.geo = _L.hpc_geometry(self.maxlevel, (C.c_int * 3)(*self.enb), (C.c_double * 3)(*map(float, x0)),
                                    (C.c_int * 3)(*map(int, roi)))
         h = C.c_void_p()
-        _L.check("hpc_create", self.lib.hpc_create(C.byref(h), C.byref(self.geo), int(device)))
-        self.h = h
         self.dims = [tuple(e * (1 << l) + 1 for e in self.enb) for l in range(self.maxlevel + 1)]
+        self.slab = None
+        if slab is None:
+            _L.check("hpc_create", self.lib.hpc_create(C.byref(h), C.byref(self.geo), int(device)))
+        else:
+            nranks, rank = int(slab[0]), int(slab[1])
+            _L.check("hpc_create_slab", self.lib.hpc_create_slab(C.byref(h), C.byref(self.geo), int(device), nranks,
+                                                                 rank))
+            self.slab = (nranks, rank)
+            self.plans = [slab_level(self.maxlevel, self.enb, nranks, rank, l) for l in range(self.maxlevel + 1)]
+            self.dims = [(d[0], d[1], p[0]) for d, p in zip(self.dims, self.plans)]
+        self.h = h
 
     # ------------------------------------------------------------ lifetime
     def close(self):

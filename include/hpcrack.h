@@ -347,6 +347,50 @@ int hpc_batch_timing(hpc_batch* batch, int on, double* out);
  * scratch: calls that overlap on the GPU race. */
 int hpc_dmax_noalloc(const double* d, const double* d_old, long long n, double* out, void* stream);
 
+/* ---------------- one specimen split along z over ranks ---------------- */
+/* The reference's MPI domain decomposition (3-D, MPI_Cart) restricted to z, one rank per GPU or per
+ * host thread.  Replaces, for a z-split:
+ *   - the per-rank level sizes of initialize (initialization.cpp:19-134): coarsest nodes
+ *     q = (kk + 1) / nranks per rank, the last rank also the remainder, one ghost plane on every
+ *     side that has a neighbour;
+ *   - the rank's coordinates, get_coordinate (boundary_conditions.cpp:13-18): the Dirichlet sets,
+ *     the image planes and the pre-crack are those of the whole specimen;
+ *   - realdomain (realdomain.h:17-40): vv_product / grid_norm (pcg_utilities.cpp:16-58), d_max,
+ *     delta_d_max (phase_field_max_search.cpp:17-53) and the reaction sum
+ *     (mechanical_right_hnd.cpp:40-59) run over owned planes and are combined over the ranks;
+ *   - SendRecv (mpi_communications.h:24-47) in z at the reference's call sites: after the PCG
+ *     direction (mechanical_pcg.cpp:278, phase_field_pcg.cpp:180), injection
+ *     (multigrid_intergrid.cpp:99,116), before the restriction (:356,393), after prolongation
+ *     (:531,547) and after the coarse material (image_input.cpp:269,
+ *     material_coarse_element.cpp:98,114).
+ * A slab context holds only its planes: hpc_upload / hpc_download / hpc_level_dims see the local
+ * nx * ny * nz_local arrays (ghost planes included).  Every call that solves, transfers or reduces
+ * is a collective step: all ranks make the same calls in the same order.  A slab runs the FAS
+ * V-cycles of the reference (mech_solver HPC_MECH_FAS; the flexible-PCG forms and hpc_batch_step
+ * return HPC_ERR_ARG), without the one-block coarsest solve, graphs or strip autotuning.
+ * Out of scope: x and y splits. */
+/* Host only, no device: out4 = {local nz, global z index of local plane 0, first owned plane, one
+ * past the last owned plane} of rank `rank` of `nranks` on `level`; HPC_ERR_ARG if a rank would own
+ * no coarsest plane. */
+int hpc_slab_level(const hpc_geometry* geo, int nranks, int rank, int level, int* out4);
+/* A context for rank `rank` of `nranks`; it joins a transport before its first collective step. */
+int hpc_create_slab(hpc_ctx** out, const hpc_geometry* geo, int device, int nranks, int rank);
+/* In-process transport: the ranks are host threads of this process (each calling its own context,
+ * all at once), on one device or several; planes move by device copies, reductions are combined
+ * on the host in rank order (every rank gets the same bits).  A wait for a rank that does not
+ * arrive ends after 120 s with HPC_ERR_CUDA; hpc_slab_group_abort ends every wait at once.  The
+ * group outlives its member contexts. */
+typedef struct hpc_slab_group hpc_slab_group;
+int hpc_slab_group_create(hpc_slab_group** out, int nranks);
+int hpc_slab_group_join(hpc_slab_group* group, hpc_ctx* ctx);
+int hpc_slab_group_abort(hpc_slab_group* group);
+int hpc_slab_group_destroy(hpc_slab_group* group);
+/* NCCL transport, one process per GPU: rank 0 makes the id, the caller hands it to every rank (a
+ * torch.distributed broadcast, a file), each rank joins with its context (ncclCommInitRank: all
+ * ranks at once).  NCCL is loaded at run time (libnccl.so.2); HPC_ERR_NODEVICE without it. */
+int hpc_nccl_unique_id(unsigned char* out128);
+int hpc_slab_join_nccl(hpc_ctx* ctx, const unsigned char* id128);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,175 @@
+"""One specimen split along z over slab ranks against the same specimen in one context (GPU).
+
+The ranks are slab contexts of this process on one device, one host thread each, joined by the
+library's in-process transport (SlabGroup); the decomposition, ghost exchanges and reductions are the
+ones a multi-GPU run makes over NCCL.  The whole-specimen context runs the same per-iteration coarsest
+solve (hpc_set_fused_coarsest(0)), so the two differ only in the order of the reductions' sums:
+operators and transfers agree to rounding, staggered increments within 1e-10 with equal V-cycle counts
+(on pre-cracked specimens from the second increment on within the spreads of tests/cases.py).  A
+one-rank slab over NCCL reproduces the whole specimen bit for bit.
+"""
+import os
+import time
+
+import numpy as np
+import pytest
+
+from hpcrack_b200 import lib as L
+from hpcrack_b200 import microstructure as ms
+from hpcrack_b200.slab import SlabGroup, join_nccl, nccl_unique_id
+from hpcrack_b200.solver import MECH_MIXED, Batch, Hierarchy, step_params
+from cases import (BULK, CRACK_CYCLE_SLACK, CRACK_F_TOL, CRACK_U_TOL, D, FD, FU, GC, G, H, R, RU, U, UOLD,
+                   load_random, load_workload, rel)
+
+pytestmark = pytest.mark.gpu
+
+
+def _whole(maxlevel, enb, x0=(0.0, 0.0, 0.0)):
+    h = Hierarchy(maxlevel, enb, x0=x0)
+    h.set_fused_coarsest(False)
+    return h
+
+
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_slab_operators_transfers_and_reductions_match_the_whole_specimen(nranks):
+    ml, enb = 2, (2, 3, 4)  # 9 x 13 x 17 finest nodes; 3 ranks: 2 / 3 / 4 coarsest planes, with ghosts
+    whole = _whole(ml, enb)
+    split = SlabGroup(ml, enb, nranks)
+    try:
+        load_random([whole, split], ml, enb, seed=3)
+        for l in range(ml + 1):
+            for impl in (whole, split):
+                impl.internal_force(l, U, RU, 1e-5)
+            assert rel(split.get(RU, l), whole.get(RU, l)) < 1e-14, l
+            for impl in (whole, split):
+                impl.prem_u(l, RU, 1e-5)
+            assert rel(split.get(RU, l), whole.get(RU, l)) < 1e-14, l
+            for impl in (whole, split):
+                impl.fld(l, D, FD, 2.0)
+            assert rel(split.get(FD, l), whole.get(FD, l)) < 1e-14, l
+            # reductions over owned planes, combined over the ranks
+            a, b = whole.initial_residual_u(l, 1e-5), split.initial_residual_u(l, 1e-5)
+            assert abs(a - b) <= 1e-13 * abs(a), (l, a, b)
+            a, b = whole.initial_residual_d(l, 2.0), split.initial_residual_d(l, 2.0)
+            assert abs(a - b) <= 1e-13 * abs(a), (l, a, b)
+        for lf in range(1, ml + 1):
+            for comp in range(3):
+                for impl in (whole, split):
+                    impl.solution_injection(U, comp, lf)
+                assert np.array_equal(split.get(U, lf - 1)[comp], whole.get(U, lf - 1)[comp]), (lf, comp)
+                for impl in (whole, split):
+                    impl.coarsen_f_standard(RU, FU, UOLD, comp, lf)
+                assert rel(split.get(RU, lf - 1)[comp], whole.get(RU, lf - 1)[comp]) < 1e-14, (lf, comp)
+                for impl in (whole, split):
+                    impl.refine_standard(U, RU, UOLD, comp, lf)
+                assert rel(split.get(U, lf)[comp], whole.get(U, lf)[comp]) < 1e-14, (lf, comp)
+        for impl in (whole, split):
+            impl.vr_all_level(BULK)
+            impl.coarse_vr(G)
+        for l in range(ml + 1):
+            assert rel(split.get(BULK, l), whole.get(BULK, l)) < 1e-14, l
+            assert rel(split.get(G, l), whole.get(G, l)) < 1e-14, l
+        # one smoother call of pcg_u (direction exchanged after every update)
+        for impl in (whole, split):
+            impl.prem_u(ml, RU, 1e-5)
+        _, fw = whole.pcg_u(ml, 1e-5, 1.0, 6, 1, 1.0)
+        _, fs = split.pcg_u(ml, 1e-5, 1.0, 6, 1, 1.0)
+        assert rel(split.get(U, ml), whole.get(U, ml)) < 1e-12
+        assert split.d_max() == whole.d_max() and split.delta_d_max() == whole.delta_d_max()
+    finally:
+        whole.close()
+        split.close()
+
+
+CASES = [("small33", 2, 3), ("crack33", 2, 3), ("crack33", 3, 2), ("box65x33x33", 4, 2)]
+
+
+def _workload(name):
+    if name.startswith("box"):
+        return ms.inclusion_workload(name, (65, 33, 33), 101, 0.2, None, 2)
+    return ms.make_workload(name)
+
+
+@pytest.mark.parametrize("name,nranks,steps", CASES, ids=[f"{n}-{r}ranks" for n, r, _ in CASES])
+def test_slab_increments_match_the_whole_specimen(name, nranks, steps):
+    w = _workload(name)
+    whole = _whole(w.maxlevel, w.element_nb, w.x_start)
+    split = SlabGroup(w.maxlevel, w.element_nb, nranks, x0=w.x_start)
+    try:
+        load_workload([whole, split], w)
+        Lf = w.maxlevel
+        for l in range(Lf + 1):
+            for f in (BULK, G, GC):
+                assert rel(split.get(f, l), whole.get(f, l)) == 0.0, (l, f)
+        assert rel(split.get(H, 0), whole.get(H, 0)) < 1e-15
+        cracked = w.crack is not None
+        kw = dict(ut0=w.ut0, dU=w.du, mech_tol=w.mech_tol, pf_tol=w.pf_tol)
+        for t in range(steps):
+            ow = whole.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, **kw)
+            osl = split.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, **kw)
+            assert ow[5] == osl[5] and ow[7] == osl[7], (t, ow, osl)
+            if t == 0 or not cracked:
+                assert ow[4] == osl[4] and ow[6] == osl[6], (t, ow, osl)
+                assert rel(split.get(U, Lf), whole.get(U, Lf)) < 1e-10, t
+                assert abs(ow[1] - osl[1]) <= 1e-10 * abs(ow[1]), (t, ow, osl)
+            else:
+                assert abs(ow[4] - osl[4]) <= CRACK_CYCLE_SLACK, (t, ow, osl)
+                assert rel(split.get(U, Lf), whole.get(U, Lf)) < CRACK_U_TOL[w.mech_tol], t
+                assert abs(ow[1] - osl[1]) <= CRACK_F_TOL[w.mech_tol] * abs(ow[1]), t
+            assert rel(split.get(D, Lf), whole.get(D, Lf)) < 1e-10, t
+            assert rel(split.get(H, Lf), whole.get(H, Lf)) < 1e-10, t
+            assert abs(ow[2] - osl[2]) <= 1e-12 and abs(ow[3] - osl[3]) <= 1e-12 * max(abs(ow[3]), 1.0), t
+        if cracked:
+            assert ow[5] >= 1  # the phase field moved
+    finally:
+        whole.close()
+        split.close()
+
+
+def test_one_rank_slab_over_nccl_reproduces_the_whole_specimen():
+    os.environ.setdefault("NCCL_SOCKET_IFNAME", "lo")
+    w = ms.make_workload("crack33")
+    whole = _whole(w.maxlevel, w.element_nb, w.x_start)
+    one = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start, slab=(1, 0))
+    try:
+        join_nccl(one, nccl_unique_id())
+        load_workload([whole, one], w)
+        kw = dict(ut0=w.ut0, dU=w.du, mech_tol=w.mech_tol, pf_tol=w.pf_tol)
+        for t in range(2):
+            ow = whole.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, **kw)
+            oo = one.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, **kw)
+            assert ow == oo, (t, ow, oo)
+        for f in (U, D, H):
+            assert np.array_equal(one.get(f, w.maxlevel), whole.get(f, w.maxlevel)), f
+    finally:
+        whole.close()
+        one.close()
+
+
+def test_slab_refusals_and_abort():
+    w = ms.make_workload("small17")
+    split = SlabGroup(w.maxlevel, w.element_nb, 2, x0=w.x_start)
+    try:
+        load_workload([split], w)
+        with pytest.raises(L.HpcError):
+            split.step(0, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du, mech_solver=MECH_MIXED)
+        with pytest.raises(L.HpcError):
+            split.set_fused_coarsest(True)
+        with pytest.raises(L.HpcError):
+            split.set_autotune(True)
+        p = step_params(0, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du)
+        with Batch() as b, pytest.raises(L.HpcError):
+            b.step([split.ranks[0]], [p])
+
+        # a rank that fails before a collective step ends the other rank's wait (no hang, an error)
+        def fn(h):
+            if h.slab[1] == 1:
+                raise RuntimeError("rank 1 failed")
+            return h.initial_residual_u(w.maxlevel, w.small_k)
+
+        t0 = time.time()
+        with pytest.raises(RuntimeError, match="rank 1 failed"):
+            split.run(fn)
+        assert time.time() - t0 < 60
+    finally:
+        split.close()

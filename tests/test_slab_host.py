@@ -1,0 +1,233 @@
+"""CPU tests of the z-slab decomposition (one specimen split along z over ranks).
+
+1. hpc_slab_level (host only) against the reference's own per-rank formulas, restated here:
+   initialize's node counts (initialization.cpp:50-72 for the coarsest level, :92-125 for the finer
+   ones), get_coordinate (boundary_conditions.cpp:13-18) and realdomain (realdomain.h:17-40).
+2. The properties the library's kernels rely on: the owned planes tile the specimen in rank order on
+   every level, each ghost plane is a neighbour's edge plane, coarse plane kc lies on fine plane
+   2 kc + zsh with zsh in {0, -1}, owned coarse nodes fall on owned fine nodes.
+3. A world-size-2 gloo run of the exchange schedule the library follows (slab.cu): Jacobi-PCG with a
+   7-point operator on two slabs, the direction's ghost planes exchanged after every direction update
+   (plane 1 to the rank below, plane nz-2 to the rank above) and the dot products summed over owned
+   planes and all-reduced, against the same PCG on the whole grid.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from hpcrack_b200 import lib as L
+from hpcrack_b200.solver import slab_level
+
+
+# ---------------------------------------------------------------- the reference's formulas
+def ref_nbcolo(kk0, npz, coord, maxlevel):
+    """nbcoloz per level (initialization.cpp:50-72, :92-125)."""
+    q = (kk0 + 1) // npz
+    if npz == 1:
+        n = kk0 + 1
+    else:
+        n = q + 2
+        if coord == 0:
+            n = q + 1
+        if coord == npz - 1:
+            n = q + (kk0 + 1) % npz + 1
+    out = []
+    for _ in range(maxlevel + 1):
+        out.append(n)
+        if npz == 1 or coord == 0:
+            n = 2 * (n - 1) + 1
+        elif coord == npz - 1:
+            n = 2 * (n - 1)
+        else:
+            n = 2 * (n - 2) + 2
+    return out
+
+
+def ref_global_index(coord, npz, total, nbcolo, index):
+    """get_coordinate (boundary_conditions.cpp:13-18) with origin 0 and spacing 1."""
+    if coord == 0:
+        return index
+    if coord == npz - 1:
+        return total - nbcolo + 1 + index
+    return coord * (nbcolo - 2) + index - 1
+
+
+def ref_realdomain(n, coord, npz):
+    """realdomain (realdomain.h:17-40) along one axis: [lo, hi)."""
+    lo, hi = 0, n
+    if npz > 1:
+        if coord == 0:
+            hi = n - 1
+        elif coord == npz - 1:
+            lo = 1
+        else:
+            lo, hi = 1, n - 1
+    return lo, hi
+
+
+CASES = [(kk0, ml, npz) for kk0 in range(1, 21) for ml in range(0, 5) for npz in range(1, 9)]
+
+
+@pytest.mark.parametrize("kk0,maxlevel,npz", CASES)
+def test_slab_plan_matches_reference_decomposition(kk0, maxlevel, npz):
+    enb = (2, 3, kk0)
+    if (kk0 + 1) // npz < 1:
+        with pytest.raises(L.HpcError):
+            slab_level(maxlevel, enb, npz, 0, 0)
+        return
+    plans = [[slab_level(maxlevel, enb, npz, r, l) for l in range(maxlevel + 1)] for r in range(npz)]
+    for r in range(npz):
+        ns = ref_nbcolo(kk0, npz, r, maxlevel)
+        for l in range(maxlevel + 1):
+            nz, zb, lo, hi = plans[r][l]
+            assert nz == ns[l], (r, l)
+            assert zb == ref_global_index(r, npz, kk0 << l, nz, 0), (r, l)
+            assert (lo, hi) == ref_realdomain(nz, r, npz), (r, l)
+    for l in range(maxlevel + 1):
+        nzg = (kk0 << l) + 1
+        # owned planes tile [0, nzg) in rank order
+        cur = 0
+        for r in range(npz):
+            nz, zb, lo, hi = plans[r][l]
+            assert zb + lo == cur and hi > lo
+            cur = zb + hi
+            # ghosts: one plane beyond the owned ones towards each neighbour, nothing else
+            assert lo == (1 if r > 0 else 0) and hi == (nz - 1 if r < npz - 1 else nz)
+            if r > 0:  # my plane 0 is the rank below's last owned plane (its plane nz-2)
+                nzb, zbb, _, hib = plans[r - 1][l]
+                assert zb == zbb + hib - 1 and hib == nzb - 1
+            if r < npz - 1:  # my plane nz-1 is the rank above's first owned plane (its plane 1)
+                assert zb + nz - 1 == plans[r + 1][l][1] + 1
+        assert cur == nzg
+        if l < maxlevel:
+            for r in range(npz):
+                nzc, zbc, loc, hic = plans[r][l]
+                nzf, zbf, lof, hif = plans[r][l + 1]
+                zsh = 2 * zbc - zbf
+                assert zsh in (0, -1) and (zsh == 0) == (r == 0 or npz == 1)
+                for kc in range(loc, hic):  # owned coarse nodes land on owned fine nodes
+                    assert lof <= 2 * kc + zsh < hif
+                assert 2 * (nzc - 1) + zsh <= nzf - 1  # every coarse plane's fine plane exists (or is < 0)
+
+
+def test_every_declared_slab_entry_point_is_exported():
+    lib = L.load()
+    for name in ("hpc_slab_level", "hpc_create_slab", "hpc_slab_group_create", "hpc_slab_group_join",
+                 "hpc_slab_group_abort", "hpc_slab_group_destroy", "hpc_nccl_unique_id", "hpc_slab_join_nccl"):
+        assert hasattr(lib, name), name
+
+
+# ---------------------------------------------------------------- two ranks over gloo
+torch = pytest.importorskip("torch")
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _apply(u):
+    """7-point operator 6u - sum of the neighbours, zero outside the array (z, y, x axes)."""
+    out = 6.0 * u
+    for ax in range(3):
+        out[tuple(slice(1, None) if a == ax else slice(None) for a in range(3))] -= \
+            u[tuple(slice(None, -1) if a == ax else slice(None) for a in range(3))]
+        out[tuple(slice(None, -1) if a == ax else slice(None) for a in range(3))] -= \
+            u[tuple(slice(1, None) if a == ax else slice(None) for a in range(3))]
+    return out
+
+
+def _pcg(f, iters, dot, exchange):
+    """Restarted Jacobi-PCG of mechanical_pcg.cpp:268-321 (beta = 0 first) on one array."""
+    u = np.zeros_like(f)
+    r = f - _apply(u)
+    p = np.zeros_like(f)
+    rz_old = None
+    for i in range(iters):
+        z = r / 6.0
+        rz = dot(r, z)
+        p = z if i == 0 else z + (rz / rz_old) * p
+        exchange(p)
+        w = _apply(p)
+        alpha = rz / dot(p, w)
+        u += alpha * p
+        r -= alpha * w
+        rz_old = rz
+    return u
+
+
+GEOM = dict(maxlevel=2, enb=(2, 2, 3))
+
+
+def _global_f():
+    nzg = (GEOM["enb"][2] << GEOM["maxlevel"]) + 1
+    ny = (GEOM["enb"][1] << GEOM["maxlevel"]) + 1
+    nx = (GEOM["enb"][0] << GEOM["maxlevel"]) + 1
+    return np.random.default_rng(5).standard_normal((nzg, ny, nx))
+
+
+def _worker(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        nz, zb, lo, hi = slab_level(GEOM["maxlevel"], GEOM["enb"], world, rank, GEOM["maxlevel"])
+        fg = _global_f()
+        f = fg[zb:zb + nz].copy()
+        f[:lo] = 0.0  # a rank's right-hand side only matters on its owned planes
+        f[hi:] = 0.0
+
+        def dot(a, b):
+            t = torch.tensor([float(np.sum(a[lo:hi] * b[lo:hi]))], dtype=torch.float64)
+            dist.all_reduce(t)
+            return float(t[0])
+
+        def exchange(p):
+            reqs, bufs = [], []
+            if rank > 0:
+                reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(p[1])), rank - 1))
+                bufs.append((0, torch.empty(p[0].shape, dtype=torch.float64)))
+                reqs.append(dist.irecv(bufs[-1][1], rank - 1))
+            if rank < world - 1:
+                reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(p[nz - 2])), rank + 1))
+                bufs.append((nz - 1, torch.empty(p[0].shape, dtype=torch.float64)))
+                reqs.append(dist.irecv(bufs[-1][1], rank + 1))
+            for rq in reqs:
+                rq.wait()
+            for k, b in bufs:
+                p[k] = b.numpy()
+
+        u = _pcg(f, 12, dot, exchange)
+        q.put((rank, zb, lo, hi, u[lo:hi].copy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_slab_ranks_reproduce_the_whole_grid_pcg():
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=120) for _ in procs), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    fg = _global_f()
+    whole = _pcg(fg, 12, lambda a, b: float(np.sum(a * b)), lambda p: None)
+    split = np.concatenate([u for _, _, _, _, u in res], axis=0)
+    assert [zb + lo for _, zb, lo, _, _ in res] == [0, res[0][1] + res[0][3]]
+    assert split.shape == whole.shape
+    err = np.linalg.norm(split - whole) / np.linalg.norm(whole)
+    assert err < 1e-12, err
