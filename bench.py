@@ -67,6 +67,9 @@ def parse_args():
     ap.add_argument("--no-tma", action="store_true",
                     help="stage the finest applies' node rows with per-lane cp.async instead of tensor copies "
                          "(hpc_set_tma_staging 0)")
+    ap.add_argument("--split", choices=("replicas", "slab"), default="replicas",
+                    help="replicas: one specimen per GPU (weak scaling, the default); slab: one specimen split "
+                         "along z over the GPUs, one rank each over NCCL (strong scaling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kernel-timing", action="store_true")
@@ -436,6 +439,88 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def run_slab(args, rank, world, local):
+    """--split slab: one specimen split along z over the job's ranks (hpc_create_slab, one GPU each, ghost
+    planes and reductions over NCCL): strong scaling, the same work at every N.  value = the specimen's
+    DoF-iterations / the slowest rank's device time."""
+    import torch
+    from hpcrack_b200 import microstructure as ms
+    from hpcrack_b200 import slab
+    from hpcrack_b200.solver import KC_MECH_PCG_FINEST, D, H, Hierarchy
+
+    torch.cuda.set_device(local)
+    w = workload(args)
+    nx, ny, nz = w.nodes
+    N = nx * ny * nz
+    if world > 1:
+        h = slab.from_process_group(w.maxlevel, w.element_nb, w.x_start, device=local)
+    else:  # one rank: a one-rank communicator on this host
+        os.environ.setdefault("NCCL_SOCKET_IFNAME", "lo")
+        h = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start, device=local, slab=(1, 0))
+        slab.join_nccl(h, slab.nccl_unique_id())
+    Lf = w.maxlevel
+    h.image_material(w.image, w.nodes, w.table(), w.voxel_size)
+    if w.crack:
+        Hc, dc = ms.precrack_fields(w)
+        h.set(H, Lf, slab.local_part(h, Lf, Hc))
+        h.set(D, Lf, slab.local_part(h, Lf, dc))
+        h.voigt_all_level(H)
+    stream = torch.cuda.ExternalStream(h.stream())
+    solver = MECH_SOLVERS[args.mech_solver]
+
+    def step(t):
+        return h.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du, dU_factor=w.du_factor,
+                      mech_tol=w.mech_tol, pf_tol=w.pf_tol, mech_solver=solver)
+
+    for t in range(args.warmup):
+        step(t)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    h.kernel_timing(KC_MECH_PCG_FINEST)
+    launches0 = h.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    outs = [step(args.warmup + i) for i in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    launches = h.launch_count() - launches0
+    kn, kms = h.kernel_time()
+    h.kernel_timing(-1)
+    ms_rank = e0.elapsed_time(e1)
+    max_ms = ms_rank
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms_rank], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        max_ms = float(tt.item())
+    dof_iters = sum(3.0 * N * o[6] + 1.0 * N * o[7] for o in outs)  # every rank reports the specimen's counts
+    local_nodes = nx * ny * h.dims[Lf][2]
+    h.close()
+    if rank == 0:
+        peak, src = peaks()
+        achieved = local_nodes * APPLY_BYTES_PER_NODE / (kms / max(kn, 1) / 1e3) / 1e9 if kn else None
+        cfg = workload_config(w, world, args.mech_solver)
+        plans = [slab.slab_level(w.maxlevel, w.element_nb, world, r, Lf) for r in range(world)]
+        cfg.update({"parallelism": f"slab-z{world}", "replicas": 1,
+                    "split": "z slabs of the specimen, one per rank; owned finest planes per rank: "
+                             f"{[p[3] - p[2] for p in plans]}"})
+        line = {"metric": METRIC, "value": dof_iters / (max_ms / 1e3) / 1e6, "unit": METRIC, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": cfg, "clocks": clocks, "gpu_launches": launches,
+                "roofline": ({"bound": "hbm", "kernel": "finest PCG apply on rank 0's slab", "achieved": achieved,
+                              "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": src,
+                              "bytes_per_node": APPLY_BYTES_PER_NODE, "nodes": local_nodes, "launches": kn,
+                              "avg_launch_ms": kms / kn, "traffic": None} if kn else None),
+                "e2e": None, "cpu_baseline": None,
+                "steps_detail": [{"mech_cycles": int(o[4]), "pf_cycles": int(o[5]), "F": o[1]} for o in outs]}
+        print(json.dumps(line), flush=True)
 
 
 def run_b200(args, rank, world, local):
@@ -823,6 +908,8 @@ def main():
             run_cpu_plan(args, local)
         elif args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.split == "slab":
+            run_slab(args, rank, world, local)
         else:
             run_b200(args, rank, world, local)
     finally:

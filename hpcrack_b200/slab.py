@@ -20,7 +20,7 @@ import numpy as np
 from . import lib as _L
 from .solver import VECTOR_FIELDS, Hierarchy, slab_level
 
-__all__ = ["SlabGroup", "slab_level", "nccl_unique_id", "join_nccl", "from_process_group"]
+__all__ = ["SlabGroup", "slab_level", "local_part", "nccl_unique_id", "join_nccl", "from_process_group"]
 
 
 def _planes(arr, nz_total, ny, nx, vector):
@@ -163,6 +163,15 @@ class SlabGroup:
 
 
 # ---------------------------------------------------------------- one process per GPU
+def local_part(h: Hierarchy, level, arr, vector=False):
+    """A slab rank's planes (ghost planes included) of a whole-specimen array of `level`."""
+    nx, ny, _ = h.dims[level]
+    nz, zb, _, _ = h.plans[level]
+    a = np.asarray(arr)
+    a = a.reshape((3, -1, ny, nx) if vector else (-1, ny, nx))
+    return np.ascontiguousarray(a[:, zb:zb + nz] if vector else a[zb:zb + nz]).reshape((3, -1) if vector else -1)
+
+
 def nccl_unique_id() -> bytes:
     """hpc_nccl_unique_id: the id rank 0 makes and hands to every rank."""
     lib = _L.load()
