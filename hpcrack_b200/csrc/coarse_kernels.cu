@@ -204,8 +204,9 @@ size_t coarse_smem_bytes(const LevelGeo& g) {
 
 bool coarse_pcg_fits(hpc_ctx* c, int level) {
   if (level == c->maxlevel) return false;  // the finest level's material is nodal, not element-constant
-  return coarse_smem_bytes(c->L[level]) <= 220 * 1024;
+  return coarse_pcg_fits_geo(c->L[level]);
 }
+bool coarse_pcg_fits_geo(const LevelGeo& g) { return coarse_smem_bytes(g) <= 220 * 1024; }
 
 // Shared-memory opt-in of the kernel on the current device (called by hpc_create).
 int coarse_pcg_prepare() {
@@ -213,14 +214,18 @@ int coarse_pcg_prepare() {
   return HPC_OK;
 }
 
-int launch_coarse_pcg(hpc_ctx* c, int level, double Ut, int nb) {
-  const LevelGeo& g = c->L[level];
-  const LevelFields& F = c->F[level];
+int launch_coarse_pcg_on(hpc_ctx* c, const LevelGeo& g, double* u, const double* fu, double* ru, const double* invM,
+                         const double* Ke, const double* Ge, double Ut, int nb) {
   const size_t smem = coarse_smem_bytes(g);
-  CoarseArgs a{g, F.u, F.fu, F.ru, F.preMu, F.Ke, F.Ge, Ut, nb, c->scal, S_RNORM};
+  CoarseArgs a{g, u, fu, ru, invM, Ke, Ge, Ut, nb, c->scal, S_RNORM};
   coarse_pcg_kernel<<<1, kCoarseThreads, smem, c->stream>>>(a);
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
+}
+
+int launch_coarse_pcg(hpc_ctx* c, int level, double Ut, int nb) {
+  const LevelFields& F = c->F[level];
+  return launch_coarse_pcg_on(c, c->L[level], F.u, F.fu, F.ru, F.preMu, F.Ke, F.Ge, Ut, nb);
 }
 
 }  // namespace hpc

@@ -275,7 +275,11 @@ int pf_diags(hpc_ctx* c, int top, double lc) {
 // pcg_u (mechanical_pcg.cpp:223-330) with preMu of level l already built.  Device scalars only.
 static int pcg_u_dev(hpc_ctx* c, int l, double small_k, double Ut, int nb, int t) {
   if (nb > kMaxRelax) return arg_fail("nb_relax too large");
-  if (c->fused_coarsest && l == 0 && coarse_pcg_fits(c, l)) return launch_coarse_pcg(c, l, Ut, nb);
+  if (c->fused_coarsest && l == 0) {
+    const int mode = slab_coarsest_mode(c);
+    if (mode == 1) return slab_coarsest(c, Ut, nb);
+    if (mode == 0 && coarse_pcg_fits(c, l)) return launch_coarse_pcg(c, l, Ut, nb);
+  }
   LevelFields& F = c->F[l];
   int rc;
   if ((rc = launch_bc(c, l, F.u, nullptr, 0, Ut))) return rc;  // Dirichlet_BD
@@ -1040,10 +1044,9 @@ static int create_ctx(hpc_ctx** out, const hpc_geometry* geo, int device, int nr
     return rc;
   };
   if (slab) {
-    // every solve of a slab runs its per-iteration kernels: the one-block coarsest solve and the graphs
-    // of coarse parts would need the exchanges inside them
+    // no graph replay of coarse parts on a slab: the in-process transport waits on the host inside
+    // them; the coarsest level is gathered and solved redundantly by the one-block solver
     c->use_graphs = 0;
-    c->fused_coarsest = 0;
     const int rc = slab_attach(c, nr, r);
     if (rc) return fail(rc);
   }
@@ -1220,7 +1223,6 @@ int hpc_set_tensor_apply(hpc_ctx* c, int on) {
 
 int hpc_set_fused_coarsest(hpc_ctx* c, int on) {
   if (!c) return arg_fail("null context");
-  if (c->slab && on) return arg_fail("a slab solves its coarsest level with per-iteration kernels");
   c->fused_coarsest = on != 0;
   return HPC_OK;
 }

@@ -209,6 +209,14 @@ struct SlabLevel {
 bool slab_levels(const hpc_geometry& g, int nr, int r, SlabLevel* out);
 int slab_attach(hpc_ctx* c, int nr, int r);  // a new context becomes rank r of nr
 void slab_release(hpc_ctx* c);
+// The coarsest level's pcg_u of a slab of several ranks, solved redundantly: every rank gathers the
+// whole coarsest level (its owned planes from every rank) and runs the one-block solver on it, then
+// keeps its own planes.  One exchange per visit instead of three collective steps per iteration.
+// 0: the context holds the whole coarsest level (no split, or one rank); 1: a split whose whole
+// coarsest level fits the one-block solver (slab_coarsest); 2: a split whose does not (per-iteration
+// kernels with their collective steps).
+int slab_coarsest_mode(hpc_ctx* c);
+int slab_coarsest(hpc_ctx* c, double Ut, int nb);
 
 // Launch timing: bracket a launch of class `cls` with events when that class is being timed.
 void timing_begin(hpc_ctx* c, int cls);
@@ -351,6 +359,9 @@ int upload_shape_table(const double* N64);
 bool coarse_pcg_fits(hpc_ctx* c, int level);
 int coarse_pcg_prepare();
 int launch_coarse_pcg(hpc_ctx* c, int level, double Ut, int nb);
+bool coarse_pcg_fits_geo(const LevelGeo& g);
+int launch_coarse_pcg_on(hpc_ctx* c, const LevelGeo& g, double* u, const double* fu, double* ru, const double* invM,
+                         const double* Ke, const double* Ge, double Ut, int nb);
 int tuned_shapes(int* out5, int cap);  // measured strip shapes: {nx, ny, nz, wy, cz} per entry
 
 

@@ -24,6 +24,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "internal.h"
 
@@ -50,6 +51,11 @@ struct hpc_slab_group {
   // reductions: each rank's values, double-buffered by call parity (a rank can be at most one
   // reduction ahead of another: the next one's barrier waits for all)
   double vals[2][hpc::kMaxSlabRanks][3];
+  // gathers: each rank's source arrays, published between the two barriers of a gather
+  struct GatherPub {
+    const char* src[8];
+    long long comp_bytes;
+  } gpub[hpc::kMaxSlabRanks];
 };
 
 struct NcclApi {
@@ -72,6 +78,15 @@ struct SlabState {
   ncclComm_t comm;        // NCCL transport
   double* hval;           // pinned staging of the reduced scalars
   int parity;
+  hpc::SlabLevel plan[hpc::kMaxSlabRanks];  // every rank's coarsest-level planes
+  // the whole coarsest level, gathered for the redundant solve (allocated on first use)
+  struct Coarse {
+    int ready;
+    hpc::LevelGeo g;
+    double* base;  // u, fu, ru, invM (3 components each), Ke, Ge
+    uint8_t* bz;
+    double *u, *fu, *ru, *invM, *Ke, *Ge;
+  } co;
 };
 
 namespace hpc {
@@ -234,6 +249,63 @@ int nccl_halo(hpc_ctx* c, int level, char* v, int ncomp, int elem) {
   return HPC_OK;
 }
 
+// Gather of the coarsest level: every rank's owned planes of `nf` fields (ncomp[f] components each)
+// into the whole-level arrays dst[f] (geometry gd) of every rank.
+int local_gather(hpc_ctx* c, const double* const* src, double* const* dst, const int* ncomp, int nf,
+                 const LevelGeo& gd) {
+  SlabState* s = c->slab;
+  hpc_slab_group* g = s->group;
+  const LevelGeo& L = c->L[0];
+  const long long plane = L.plane * (long long)sizeof(double);
+  HPC_CUDA(cudaStreamSynchronize(c->stream));
+  auto& mine = g->gpub[s->rank];
+  for (int f = 0; f < nf; ++f) mine.src[f] = reinterpret_cast<const char*>(src[f]);
+  mine.comp_bytes = L.n * (long long)sizeof(double);
+  int rc = group_barrier(g);
+  if (rc) return rc;
+  for (int q = 0; q < s->nr; ++q) {
+    const SlabLevel& pq = s->plan[q];
+    const auto& pub = g->gpub[q];
+    for (int f = 0; f < nf; ++f)
+      for (int m = 0; m < ncomp[f]; ++m) {
+        char* d = reinterpret_cast<char*>(dst[f]) + m * gd.n * (long long)sizeof(double) + (long long)(pq.zb + pq.lo) * plane;
+        const char* from = pub.src[f] + m * pub.comp_bytes + (long long)pq.lo * plane;
+        HPC_CUDA(cudaMemcpyAsync(d, from, (size_t)(pq.hi - pq.lo) * plane, cudaMemcpyDefault, c->stream));
+      }
+  }
+  HPC_CUDA(cudaStreamSynchronize(c->stream));
+  return group_barrier(g);
+}
+
+int nccl_gather(hpc_ctx* c, const double* const* src, double* const* dst, const int* ncomp, int nf,
+                const LevelGeo& gd) {
+  NcclApi& api = nccl();
+  SlabState* s = c->slab;
+  const LevelGeo& L = c->L[0];
+  const SlabLevel& me = s->plan[s->rank];
+  for (int f = 0; f < nf; ++f)  // this rank's own planes
+    for (int m = 0; m < ncomp[f]; ++m)
+      HPC_CUDA(cudaMemcpyAsync(dst[f] + m * gd.n + (me.zb + me.lo) * L.plane, src[f] + m * L.n + me.lo * L.plane,
+                               sizeof(double) * (size_t)(me.hi - me.lo) * L.plane, cudaMemcpyDeviceToDevice, c->stream));
+  ncclResult_t r = api.GroupStart();
+  if (r != ncclSuccess) return nccl_fail(r, "ncclGroupStart");
+  for (int f = 0; f < nf && r == ncclSuccess; ++f)
+    for (int m = 0; m < ncomp[f] && r == ncclSuccess; ++m)
+      for (int q = 0; q < s->nr && r == ncclSuccess; ++q) {
+        if (q == s->rank) continue;
+        const SlabLevel& pq = s->plan[q];
+        r = api.Send(src[f] + m * L.n + me.lo * L.plane, (size_t)(me.hi - me.lo) * L.plane, ncclFloat64, q, s->comm,
+                     c->stream);
+        if (r == ncclSuccess)
+          r = api.Recv(dst[f] + m * gd.n + (pq.zb + pq.lo) * L.plane, (size_t)(pq.hi - pq.lo) * L.plane, ncclFloat64,
+                       q, s->comm, c->stream);
+      }
+  const ncclResult_t e = api.GroupEnd();
+  if (r != ncclSuccess) return nccl_fail(r, "ncclSend/ncclRecv (gather)");
+  if (e != ncclSuccess) return nccl_fail(e, "ncclGroupEnd");
+  return HPC_OK;
+}
+
 int no_transport() {
   set_error("slab context of several ranks without a transport (hpc_slab_group_join or hpc_slab_join_nccl)");
   return HPC_ERR_ARG;
@@ -281,9 +353,68 @@ int slab_halo(hpc_ctx* c, int level, void* v, int ncomp, int elem_bytes) {
   return no_transport();
 }
 
+int slab_coarsest_mode(hpc_ctx* c) {
+  if (!c->slab || c->slab->nr == 1) return 0;
+  LevelGeo g = c->L[0];
+  g.nz = c->geo.element_nb[2] + 1;
+  return c->maxlevel > 0 && coarse_pcg_fits_geo(g) ? 1 : 2;
+}
+
+int slab_coarsest(hpc_ctx* c, double Ut, int nb) {
+  SlabState* s = c->slab;
+  auto& co = s->co;
+  const LevelGeo& L = c->L[0];
+  if (!co.ready) {
+    LevelGeo g = L;
+    g.nz = c->geo.element_nb[2] + 1;
+    g.n = g.plane * g.nz;
+    g.zb = 0;
+    g.oz0 = 0;
+    g.oz1 = g.nz;
+    g.zsh = 0;
+    std::vector<uint8_t> fz(g.nz);
+    const double* B = c->box;
+    for (int k = 0; k < g.nz; ++k) {  // the Dirichlet planes of the whole level, as hpc_create sets them
+      const double z = B[4] + k * g.hz;
+      fz[k] = (uint8_t)((z == B[4] ? 1 : 0) | (z == B[5] ? 2 : 0));
+    }
+    const size_t doubles = (size_t)g.n * 14;
+    HPC_CUDA(cudaMallocAsync((void**)&co.base, sizeof(double) * doubles + g.nz, c->stream));
+    HPC_CUDA(cudaMemsetAsync(co.base, 0, sizeof(double) * doubles, c->stream));
+    co.u = co.base;
+    co.fu = co.u + 3 * g.n;
+    co.ru = co.fu + 3 * g.n;
+    co.invM = co.ru + 3 * g.n;
+    co.Ke = co.invM + 3 * g.n;
+    co.Ge = co.Ke + g.n;
+    co.bz = reinterpret_cast<uint8_t*>(co.base + doubles);
+    HPC_CUDA(cudaMemcpyAsync(co.bz, fz.data(), g.nz, cudaMemcpyHostToDevice, c->stream));
+    HPC_CUDA(cudaStreamSynchronize(c->stream));  // fz leaves scope
+    g.bz = co.bz;
+    co.g = g;
+    co.ready = 1;
+  }
+  const LevelFields& F = c->F[0];
+  const double* src[5] = {F.u, F.fu, F.preMu, F.Ke, F.Ge};
+  double* dst[5] = {co.u, co.fu, co.invM, co.Ke, co.Ge};
+  const int nc[5] = {3, 3, 3, 1, 1};
+  int rc = s->group ? local_gather(c, src, dst, nc, 5, co.g) : s->comm ? nccl_gather(c, src, dst, nc, 5, co.g) : no_transport();
+  if (rc) return rc;
+  // the same inputs on every rank, a deterministic solver: the same whole-level solution everywhere
+  if ((rc = launch_coarse_pcg_on(c, co.g, co.u, co.fu, co.ru, co.invM, co.Ke, co.Ge, Ut, nb))) return rc;
+  for (int m = 0; m < 3; ++m) {  // this rank's planes, ghost planes included
+    HPC_CUDA(cudaMemcpyAsync(F.u + m * L.n, co.u + m * co.g.n + L.zb * L.plane, sizeof(double) * L.n,
+                             cudaMemcpyDeviceToDevice, c->stream));
+    HPC_CUDA(cudaMemcpyAsync(F.ru + m * L.n, co.ru + m * co.g.n + L.zb * L.plane, sizeof(double) * L.n,
+                             cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return HPC_OK;
+}
+
 void slab_release(hpc_ctx* c) {
   SlabState* s = c->slab;
   if (!s) return;
+  if (s->co.base) cudaFreeAsync(s->co.base, c->stream);
   if (s->group) {
     std::lock_guard<std::mutex> lock(s->group->mu);
     if (s->group->member[s->rank] == c) s->group->member[s->rank] = nullptr;
@@ -300,6 +431,14 @@ int slab_attach(hpc_ctx* c, int nr, int r) {
   s->nr = nr;
   s->rank = r;
   c->slab = s;
+  for (int q = 0; q < nr; ++q) {
+    SlabLevel lv[kMaxLevels];
+    if (!slab_levels(c->geo, nr, q, lv)) {
+      set_error("bad slab decomposition");
+      return HPC_ERR_ARG;
+    }
+    s->plan[q] = lv[0];
+  }
   HPC_CUDA(cudaMallocHost((void**)&s->hval, sizeof(double) * 4));
   return HPC_OK;
 }

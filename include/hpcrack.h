@@ -367,7 +367,10 @@ int hpc_dmax_noalloc(const double* d, const double* d_old, long long n, double* 
  * nx * ny * nz_local arrays (ghost planes included).  Every call that solves, transfers or reduces
  * is a collective step: all ranks make the same calls in the same order.  A slab runs the FAS
  * V-cycles of the reference (mech_solver HPC_MECH_FAS; the flexible-PCG forms and hpc_batch_step
- * return HPC_ERR_ARG), without the one-block coarsest solve, graphs or strip autotuning.
+ * return HPC_ERR_ARG), without graph replay or strip autotuning.  Its coarsest level is gathered on
+ * every rank and solved redundantly by the one-block solver when the whole level fits it (one
+ * exchange per visit instead of three collective steps per iteration; hpc_set_fused_coarsest(ctx, 0)
+ * selects the reference's distributed smoother there).
  * Out of scope: x and y splits. */
 /* Host only, no device: out4 = {local nz, global z index of local plane 0, first owned plane, one
  * past the last owned plane} of rank `rank` of `nranks` on `level`; HPC_ERR_ARG if a rank would own

@@ -2,11 +2,12 @@
 
 The ranks are slab contexts of this process on one device, one host thread each, joined by the
 library's in-process transport (SlabGroup); the decomposition, ghost exchanges and reductions are the
-ones a multi-GPU run makes over NCCL.  The whole-specimen context runs the same per-iteration coarsest
-solve (hpc_set_fused_coarsest(0)), so the two differ only in the order of the reductions' sums:
-operators and transfers agree to rounding, staggered increments within 1e-10 with equal V-cycle counts
-(on pre-cracked specimens from the second increment on within the spreads of tests/cases.py).  A
-one-rank slab over NCCL reproduces the whole specimen bit for bit.
+ones a multi-GPU run makes over NCCL.  The coarsest level is either gathered and solved redundantly by
+the one-block solver (the default, as the whole specimen solves it) or solved by the distributed
+per-iteration smoother (hpc_set_fused_coarsest(0) on both sides), so the two differ only in the order
+of the reductions' sums: operators and transfers agree to rounding, staggered increments within 1e-10
+with equal V-cycle counts (on pre-cracked specimens from the second increment on within the spreads of
+tests/cases.py).  A one-rank slab over NCCL reproduces the whole specimen bit for bit.
 """
 import os
 import time
@@ -24,9 +25,9 @@ from cases import (BULK, CRACK_CYCLE_SLACK, CRACK_F_TOL, CRACK_U_TOL, D, FD, FU,
 pytestmark = pytest.mark.gpu
 
 
-def _whole(maxlevel, enb, x0=(0.0, 0.0, 0.0)):
+def _whole(maxlevel, enb, x0=(0.0, 0.0, 0.0), fused=False):
     h = Hierarchy(maxlevel, enb, x0=x0)
-    h.set_fused_coarsest(False)
+    h.set_fused_coarsest(fused)
     return h
 
 
@@ -35,6 +36,7 @@ def test_slab_operators_transfers_and_reductions_match_the_whole_specimen(nranks
     ml, enb = 2, (2, 3, 4)  # 9 x 13 x 17 finest nodes; 3 ranks: 2 / 3 / 4 coarsest planes, with ghosts
     whole = _whole(ml, enb)
     split = SlabGroup(ml, enb, nranks)
+    split.set_fused_coarsest(False)
     try:
         load_random([whole, split], ml, enb, seed=3)
         for l in range(ml + 1):
@@ -81,7 +83,8 @@ def test_slab_operators_transfers_and_reductions_match_the_whole_specimen(nranks
         split.close()
 
 
-CASES = [("small33", 2, 3), ("crack33", 2, 3), ("crack33", 3, 2), ("box65x33x33", 4, 2)]
+CASES = [("small33", 2, 3, "gathered"), ("crack33", 2, 3, "gathered"), ("crack33", 3, 2, "gathered"),
+         ("crack33", 3, 2, "distributed"), ("box65x33x33", 4, 2, "distributed")]
 
 
 def _workload(name):
@@ -90,11 +93,13 @@ def _workload(name):
     return ms.make_workload(name)
 
 
-@pytest.mark.parametrize("name,nranks,steps", CASES, ids=[f"{n}-{r}ranks" for n, r, _ in CASES])
-def test_slab_increments_match_the_whole_specimen(name, nranks, steps):
+@pytest.mark.parametrize("name,nranks,steps,coarsest", CASES, ids=[f"{n}-{r}ranks-{c}" for n, r, _, c in CASES])
+def test_slab_increments_match_the_whole_specimen(name, nranks, steps, coarsest):
     w = _workload(name)
-    whole = _whole(w.maxlevel, w.element_nb, w.x_start)
+    fused = coarsest == "gathered"
+    whole = _whole(w.maxlevel, w.element_nb, w.x_start, fused=fused)
     split = SlabGroup(w.maxlevel, w.element_nb, nranks, x0=w.x_start)
+    split.set_fused_coarsest(fused)
     try:
         load_workload([whole, split], w)
         Lf = w.maxlevel
@@ -129,7 +134,7 @@ def test_slab_increments_match_the_whole_specimen(name, nranks, steps):
 def test_one_rank_slab_over_nccl_reproduces_the_whole_specimen():
     os.environ.setdefault("NCCL_SOCKET_IFNAME", "lo")
     w = ms.make_workload("crack33")
-    whole = _whole(w.maxlevel, w.element_nb, w.x_start)
+    whole = _whole(w.maxlevel, w.element_nb, w.x_start, fused=True)
     one = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start, slab=(1, 0))
     try:
         join_nccl(one, nccl_unique_id())
@@ -153,8 +158,6 @@ def test_slab_refusals_and_abort():
         load_workload([split], w)
         with pytest.raises(L.HpcError):
             split.step(0, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du, mech_solver=MECH_MIXED)
-        with pytest.raises(L.HpcError):
-            split.set_fused_coarsest(True)
         with pytest.raises(L.HpcError):
             split.set_autotune(True)
         p = step_params(0, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du)
