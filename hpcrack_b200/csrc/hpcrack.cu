@@ -431,7 +431,7 @@ static bool same_mg(const hpc_mg& a, const hpc_mg& b) {
 // `allow_capture`), replayed afterwards.  Kernel launches are counted per replay.  A graph is keyed
 // by its parameters and by `flags`, the context's kernel choices baked into its launches.
 static int graph_flags(const hpc_ctx* c) {
-  return c->tma_stage * 8 + c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active;
+  return c->autotune * 16 + c->tma_stage * 8 + c->tc_apply * 4 + c->fused_coarsest * 2 + c->gpm_active;
 }
 template <class Body>
 static int run_graphed(hpc_ctx* c, hpc_ctx::CoarseGraph& g, const hpc_mg& mg, double a, double b, bool allow_capture,

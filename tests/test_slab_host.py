@@ -231,3 +231,49 @@ def test_two_slab_ranks_reproduce_the_whole_grid_pcg():
     assert split.shape == whole.shape
     err = np.linalg.norm(split - whole) / np.linalg.norm(whole)
     assert err < 1e-12, err
+
+
+# ---------------------------------------------------------------- whole-specimen arrays <-> ranks
+class _FakeRank:
+    """Stands in for a slab context: its plan and local arrays (no device)."""
+
+    def __init__(self, maxlevel, enb, nranks, rank):
+        self.plans = [slab_level(maxlevel, enb, nranks, rank, l) for l in range(maxlevel + 1)]
+        self.dims = [((enb[0] << l) + 1, (enb[1] << l) + 1, self.plans[l][0]) for l in range(maxlevel + 1)]
+        self.slab = (nranks, rank)
+        self.store = {}
+
+    def set(self, field, level, arr):  # the layout Hierarchy.set takes: flat, or (3, n) for vectors
+        from hpcrack_b200.solver import VECTOR_FIELDS
+        a = np.array(arr, dtype=np.float64)
+        self.store[(field, level)] = a.reshape(3, -1) if field in VECTOR_FIELDS else a.ravel()
+
+    def get(self, field, level):
+        return self.store[(field, level)]
+
+
+@pytest.mark.parametrize("nranks", [1, 2, 3, 5])
+def test_slab_group_set_and_get_round_trip_whole_arrays(nranks):
+    from hpcrack_b200.slab import SlabGroup, local_part
+    from hpcrack_b200.solver import U, D
+
+    ml, enb = 2, (2, 3, 4)
+    g = object.__new__(SlabGroup)
+    g.maxlevel, g.enb, g.nranks = ml, enb, nranks
+    g.dims = [tuple(e * (1 << l) + 1 for e in enb) for l in range(ml + 1)]
+    g.ranks = [_FakeRank(ml, enb, nranks, r) for r in range(nranks)]
+    g.run = lambda fn: [fn(h) for h in g.ranks]
+    rng = np.random.default_rng(2)
+    for l in range(ml + 1):
+        n = int(np.prod(g.dims[l]))
+        d, u = rng.standard_normal(n), rng.standard_normal((3, n))
+        g.set(D, l, d)
+        g.set(U, l, u)
+        assert np.array_equal(g.get(D, l), d)
+        assert np.array_equal(g.get(U, l), u)
+        for h in g.ranks:  # every rank holds its planes, ghost planes included
+            nz, zb, _, _ = h.plans[l]
+            nx, ny = g.dims[l][:2]
+            assert np.array_equal(h.get(D, l), d.reshape(-1, ny, nx)[zb:zb + nz].ravel())
+            assert np.array_equal(h.get(D, l), local_part(h, l, d))
+            assert np.array_equal(h.get(U, l), local_part(h, l, u, vector=True))
