@@ -1044,8 +1044,8 @@ static int create_ctx(hpc_ctx** out, const hpc_geometry* geo, int device, int nr
     return rc;
   };
   if (slab) {
-    // no graph replay of coarse parts on a slab: the in-process transport waits on the host inside
-    // them; the coarsest level is gathered and solved redundantly by the one-block solver
+    // no graph replay of coarse parts until the slab joins NCCL (hpc_slab_join_nccl): the in-process
+    // transport waits on the host inside them; the coarsest level is gathered and solved redundantly
     c->use_graphs = 0;
     const int rc = slab_attach(c, nr, r);
     if (rc) return fail(rc);
@@ -1159,6 +1159,15 @@ int hpc_destroy(hpc_ctx* c) {
   if (!c) return HPC_OK;
   cudaSetDevice(c->device);
   vtk_release(c);
+  // graphs first: a slab's may hold NCCL calls of the communicator slab_release destroys
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->gmech.valid) cudaGraphExecDestroy(c->gmech.exec);
+  if (c->gpf.valid) cudaGraphExecDestroy(c->gpf.exec);
+  if (c->g32.valid) cudaGraphExecDestroy(c->g32.exec);
+  for (auto& gf : c->gfcg)
+    if (gf.valid) cudaGraphExecDestroy(gf.exec);
+  c->gmech.valid = c->gpf.valid = c->g32.valid = 0;
+  for (auto& gf : c->gfcg) gf.valid = 0;
   slab_release(c);
   for (int l = 0; l <= c->maxlevel && l < kMaxLevels; ++l) {
     LevelFields& F = c->F[l];
@@ -1185,11 +1194,6 @@ int hpc_destroy(hpc_ctx* c) {
   pinned_release(c->hscal);
   for (int i = 0; i < 2 * c->tev_cap; ++i) cudaEventDestroy(c->tev[i]);
   delete[] c->tev;
-  if (c->gmech.valid) cudaGraphExecDestroy(c->gmech.exec);
-  if (c->gpf.valid) cudaGraphExecDestroy(c->gpf.exec);
-  if (c->g32.valid) cudaGraphExecDestroy(c->g32.exec);
-  for (auto& gf : c->gfcg)
-    if (gf.valid) cudaGraphExecDestroy(gf.exec);
   if (c->ck.stream) cudaStreamSynchronize(c->ck.stream);
   if (c->ck.dev) cudaFree(c->ck.dev);
   if (c->ck.host) cudaFreeHost(c->ck.host);

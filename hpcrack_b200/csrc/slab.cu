@@ -546,6 +546,9 @@ int hpc_slab_join_nccl(hpc_ctx* c, const unsigned char* id128) {
   const ncclResult_t r = api.CommInitRank(&comm, c->slab->nr, id, c->slab->rank);
   if (r != ncclSuccess) return nccl_fail(r, "ncclCommInitRank");
   c->slab->comm = comm;
+  // NCCL's calls are enqueued on the stream without host waits, so the coarse parts of the cycles
+  // may be captured into graphs with them inside (the first cycle, uncaptured, sets up the peers)
+  c->use_graphs = 1;
   return HPC_OK;
 }
 

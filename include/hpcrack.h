@@ -367,7 +367,8 @@ int hpc_dmax_noalloc(const double* d, const double* d_old, long long n, double* 
  * nx * ny * nz_local arrays (ghost planes included).  Every call that solves, transfers or reduces
  * is a collective step: all ranks make the same calls in the same order.  A slab runs the FAS
  * V-cycles of the reference (mech_solver HPC_MECH_FAS; the flexible-PCG forms and hpc_batch_step
- * return HPC_ERR_ARG), without graph replay or strip autotuning.  Its coarsest level is gathered on
+ * return HPC_ERR_ARG), without strip autotuning; the coarse parts of its cycles replay as CUDA graphs
+ * over NCCL (the NCCL calls captured inside), not over the in-process transport.  Its coarsest level is gathered on
  * every rank and solved redundantly by the one-block solver when the whole level fits it (one
  * exchange per visit instead of three collective steps per iteration; hpc_set_fused_coarsest(ctx, 0)
  * selects the reference's distributed smoother there).
