@@ -1195,6 +1195,7 @@ static int run_mech_tc(hpc_ctx* c, const MechKT<float>& k) {
 // Single-precision element operator of the precision form's V-cycle: the same kernels on the FP32
 // mirror of a level (LevelF32); residual, PCG apply and FAS right-hand side epilogues.
 int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
+  if (m.epi == EPI_FAS) HPC_SLAB_HALO(c, m.fine_level, m.rf, 3, sizeof(float));
   MechKT<float> k{};
   const LevelF32& F = c->F32[m.level];
   const LevelGeo& g = c->L[m.level];
@@ -1222,8 +1223,9 @@ int launch_mech_f32(hpc_ctx* c, const MechCall32& m) {
   k.red = make_red(c, m.s_out0, m.s_out1, m.s_out2);
   k.err = c->scal + S_ERR;
   const bool fin = m.finest;
-  // tensor-core contraction (hpc_set_tensor_apply): isotropic levels, Gauss-point moduli at the finest
-  if (c->tc_apply && iso(g) && (!fin || k.gpm)) {
+  // tensor-core contraction (hpc_set_tensor_apply): isotropic levels, Gauss-point moduli at the finest;
+  // not on a slab (its epilogue sums every plane)
+  if (c->tc_apply && !c->slab && iso(g) && (!fin || k.gpm)) {
     switch (m.epi) {
       case EPI_PLAIN: return fin ? run_mech_tc<true, EPI_PLAIN>(c, k) : run_mech_tc<false, EPI_PLAIN>(c, k);
       case EPI_RESIDUAL: return fin ? run_mech_tc<true, EPI_RESIDUAL>(c, k) : run_mech_tc<false, EPI_RESIDUAL>(c, k);

@@ -839,7 +839,6 @@ int fcg_iteration(hpc_ctx* c, const hpc_mg& mg, double small_k, int k, bool mixe
 // iteration), *fin_iters = finest smoother iterations inside them.
 static int u_entire_fcg_dev(hpc_ctx* c, const hpc_mg& mg, double small_k, double Ut, int t, double mech_tol,
                             int* cycles, long long* fin_iters, bool mixed) {
-  if (c->slab) return arg_fail("a slab runs the reference's FAS V-cycles (mech_solver HPC_MECH_FAS)");
   int rc;
   const int L = c->maxlevel;
   LevelFields& F = c->F[L];

@@ -191,6 +191,7 @@ static int launch_fcg_dir_t(hpc_ctx* c, int level, const TZ* z, double* p, bool 
   fcg_dir_kernel<TZ><<<row_grid(g), kRowThreads, 0, c->stream>>>(g, z, p, first ? 1 : 0, c->scal, s_delta, s_gamma,
                                                                 s_delta_prev);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, level, p, 3, sizeof(double));  // the apply of p reads its ghost planes
   return HPC_OK;
 }
 int launch_fcg_dir(hpc_ctx* c, int level, const double* z, double* p, bool first, int s_delta, int s_gamma,
@@ -981,8 +982,12 @@ int launch_mech_update_f32(hpc_ctx* c, int level, int s_num, int s_den, int s_rz
   const LevelF32& F = c->F32[level];
   const long long pairs = (long long)(g.px / 2) * g.ny * g.nz;
   const int grid = (int)std::min<long long>((pairs + kRowThreads - 1) / kRowThreads, (long long)num_sms_v() * 8);
-  mech_update_kernel<float><<<grid, kRowThreads, 0, c->stream>>>(g, F.u, F.ru, F.p, F.w, F.invM, s_num, s_den,
-                                                                  make_red(c, s_rz_next, s_rn, -1));
+  if (c->slab)
+    mech_update_kernel<float, true><<<grid, kRowThreads, 0, c->stream>>>(g, F.u, F.ru, F.p, F.w, F.invM, s_num, s_den,
+                                                                       make_red(c, s_rz_next, s_rn, -1));
+  else
+    mech_update_kernel<float, false><<<grid, kRowThreads, 0, c->stream>>>(g, F.u, F.ru, F.p, F.w, F.invM, s_num,
+                                                                        s_den, make_red(c, s_rz_next, s_rn, -1));
   HPC_CHECK_LAUNCH(c);
   return HPC_OK;
 }
@@ -992,6 +997,7 @@ int launch_dir_update_f32(hpc_ctx* c, int level, bool first, int s_rz, int s_rz_
   dir_update_kernel<float><<<row_grid(g), kRowThreads, 0, c->stream>>>(g, 3, F.ru, F.invM, F.p, first ? 1 : 0,
                                                                        c->scal, s_rz, s_rz_prev);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, level, F.p, 3, sizeof(float));
   return HPC_OK;
 }
 int launch_bc_zero_f32(hpc_ctx* c, int level, float* v) {
@@ -1004,12 +1010,15 @@ int launch_inject_u_f32(hpc_ctx* c, int lf) {
   inject_u_kernel<float><<<row_grid(c->L[lf - 1]), kRowThreads, 0, c->stream>>>(
       c->L[lf - 1], c->L[lf], c->F32[lf].u, c->F32[lf - 1].u, c->F32[lf - 1].uold, 0.0f);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, lf - 1, c->F32[lf - 1].u, 3, sizeof(float));
+  HPC_SLAB_HALO(c, lf - 1, c->F32[lf - 1].uold, 3, sizeof(float));
   return HPC_OK;
 }
 int launch_prolong_f32(hpc_ctx* c, int lf) {
   prolong_kernel<float><<<row_grid(c->L[lf]), kRowThreads, 0, c->stream>>>(
       c->L[lf - 1], c->L[lf], c->F32[lf - 1].u, c->F32[lf - 1].uold, c->F32[lf].u, 3, 1, 0.0f);
   HPC_CHECK_LAUNCH(c);
+  HPC_SLAB_HALO(c, lf, c->F32[lf].u, 3, sizeof(float));
   return HPC_OK;
 }
 }  // namespace hpc
@@ -1034,7 +1043,8 @@ __global__ void residual_zero_f32_kernel(LevelGeo g, const float* f, const float
       const long long o = n + (long long)m * g.n;
       const float rv = fix[m] ? 0.f : f[o];
       r[o] = rv;
-      rz = fma((double)rv, (double)(rv * invM[o]), rz);
+      const double s1 = fma((double)rv, (double)(rv * invM[o]), rz);
+      rz = owned_plane(g, kz) ? s1 : rz;
     }
   }
   double v[1] = {rz};

@@ -365,9 +365,9 @@ int hpc_dmax_noalloc(const double* d, const double* d_old, long long n, double* 
  *     material_coarse_element.cpp:98,114).
  * A slab context holds only its planes: hpc_upload / hpc_download / hpc_level_dims see the local
  * nx * ny * nz_local arrays (ghost planes included).  Every call that solves, transfers or reduces
- * is a collective step: all ranks make the same calls in the same order.  A slab runs the FAS
- * V-cycles of the reference (mech_solver HPC_MECH_FAS; the flexible-PCG forms and hpc_batch_step
- * return HPC_ERR_ARG), without strip autotuning; the coarse parts of its cycles replay as CUDA graphs
+ * is a collective step: all ranks make the same calls in the same order.  A slab runs every
+ * mech_solver of hpc_step (hpc_batch_step returns HPC_ERR_ARG; the precision form's element
+ * contraction stays on the CUDA cores), without strip autotuning; the coarse parts of its cycles replay as CUDA graphs
  * over NCCL (the NCCL calls captured inside), not over the in-process transport.  Its coarsest level is gathered on
  * every rank and solved redundantly by the one-block solver when the whole level fits it (one
  * exchange per visit instead of three collective steps per iteration; hpc_set_fused_coarsest(ctx, 0)

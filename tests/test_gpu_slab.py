@@ -18,7 +18,7 @@ import pytest
 from hpcrack_b200 import lib as L
 from hpcrack_b200 import microstructure as ms
 from hpcrack_b200.slab import SlabGroup, join_nccl, nccl_unique_id
-from hpcrack_b200.solver import MECH_MIXED, Batch, Hierarchy, step_params
+from hpcrack_b200.solver import MECH_FCG, MECH_MIXED, Batch, Hierarchy, precision_mg, step_params
 from cases import (BULK, CRACK_CYCLE_SLACK, CRACK_F_TOL, CRACK_U_TOL, D, FD, FU, GC, G, H, R, RU, U, UOLD,
                    load_random, load_workload, rel)
 
@@ -131,6 +131,32 @@ def test_slab_increments_match_the_whole_specimen(name, nranks, steps, coarsest)
         split.close()
 
 
+@pytest.mark.parametrize("name,solver", [("small33", MECH_MIXED), ("crack33", MECH_MIXED), ("small33", MECH_FCG)],
+                         ids=["small33-mixed", "crack33-mixed", "small33-fcg"])
+def test_slab_flexible_forms_match_the_whole_specimen(name, solver):
+    """The flexible PCG (FP64 V-cycle, or the precision form's FP32 V-cycle) on 2 slab ranks against the
+    whole specimen: both solve each increment to |r|/|f| <= 1e-8, the FP32 cycle amplifies the
+    different order of the sums, so the bar is the one the forms meet against each other (1e-6)."""
+    w = ms.make_workload(name)
+    mg_u = precision_mg(w.maxlevel, w.element_nb, w.mg_u[4])
+    whole = Hierarchy(w.maxlevel, w.element_nb, x0=w.x_start)
+    split = SlabGroup(w.maxlevel, w.element_nb, 2, x0=w.x_start)
+    try:
+        load_workload([whole, split], w)
+        Lf = w.maxlevel
+        kw = dict(ut0=w.ut0, dU=w.du, mech_tol=w.mech_tol, pf_tol=w.pf_tol, mech_solver=solver)
+        for t in range(2):
+            ow = whole.step(t, mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, **kw)
+            osl = split.step(t, mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, **kw)
+            assert abs(ow[4] - osl[4]) <= 1 and abs(ow[5] - osl[5]) <= 1, (t, ow, osl)
+            for f in (U, D, H):
+                assert rel(split.get(f, Lf), whole.get(f, Lf)) < 1e-6, (t, f)
+            assert abs(ow[1] - osl[1]) <= 1e-6 * abs(ow[1]), (t, ow, osl)
+    finally:
+        whole.close()
+        split.close()
+
+
 def test_one_rank_slab_over_nccl_reproduces_the_whole_specimen():
     os.environ.setdefault("NCCL_SOCKET_IFNAME", "lo")
     w = ms.make_workload("crack33")
@@ -156,8 +182,6 @@ def test_slab_refusals_and_abort():
     split = SlabGroup(w.maxlevel, w.element_nb, 2, x0=w.x_start)
     try:
         load_workload([split], w)
-        with pytest.raises(L.HpcError):
-            split.step(0, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du, mech_solver=MECH_MIXED)
         with pytest.raises(L.HpcError):
             split.set_autotune(True)
         p = step_params(0, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du)
