@@ -277,3 +277,27 @@ def test_slab_group_set_and_get_round_trip_whole_arrays(nranks):
             assert np.array_equal(h.get(D, l), d.reshape(-1, ny, nx)[zb:zb + nz].ravel())
             assert np.array_equal(h.get(D, l), local_part(h, l, d))
             assert np.array_equal(h.get(U, l), local_part(h, l, u, vector=True))
+
+
+def test_slab_group_run_aborts_and_reraises_the_failing_rank():
+    """SlabGroup.run: every rank's call runs in its own thread; a rank that raises aborts the group
+    (no device here: aborting a null group is a refused call, not a crash) and its own exception is
+    re-raised, not the errors of ranks whose waits the abort ended."""
+    from hpcrack_b200.slab import SlabGroup
+
+    g = object.__new__(SlabGroup)
+    g.lib = L.load()
+    g.group = None
+    g.ranks = [_FakeRank(1, (2, 2, 4), 3, r) for r in range(3)]
+
+    def fn(h):
+        r = h.slab[1]
+        if r == 1:
+            raise ValueError("rank 1 failed")
+        if r == 2:
+            raise RuntimeError("slab group aborted by another rank")
+        return r
+
+    with pytest.raises(ValueError, match="rank 1 failed"):
+        g.run(fn)
+    assert g.run(lambda h: h.slab[1] * 10) == [0, 10, 20]
