@@ -135,16 +135,20 @@ static void host_geometry(const hpc_geometry& g, double box[6], HostLevel* lv) {
   }
 }
 
-static bool geometry_ok(const hpc_geometry* g) {
+// The geometry of rank r of nr along z (one rank: the whole specimen).
+static bool geometry_ok(const hpc_geometry* g, int nr = 1, int r = 0) {
   if (!g || g->maxlevel < 0 || g->maxlevel >= kMaxLevels) return false;
   for (int a = 0; a < 3; ++a)
     if (g->element_nb[a] < 1 || g->roi_start[a] < 0) return false;
   // finest node count per axis must stay a sane int
   for (int a = 0; a < 3; ++a)
     if ((double)g->element_nb[a] * std::pow(2.0, g->maxlevel) > 65000.0) return false;
-  // node-parallel kernels index a level with 32-bit arithmetic: padded node count below 2^31
-  double nodes = 1.0;
-  for (int a = 0; a < 3; ++a) nodes *= (double)g->element_nb[a] * std::pow(2.0, g->maxlevel) + 1.0 + (a == 0 ? 3 : 0);
+  SlabLevel sl[kMaxLevels];
+  if (!slab_levels(*g, nr, r, sl)) return false;
+  // node-parallel kernels index a level with 32-bit arithmetic: padded node count of the planes this
+  // context holds below 2^31 (a split lets a specimen exceed that, each rank's slab may not)
+  double nodes = (double)sl[g->maxlevel].nz;
+  for (int a = 0; a < 2; ++a) nodes *= (double)g->element_nb[a] * std::pow(2.0, g->maxlevel) + 1.0 + (a == 0 ? 3 : 0);
   if (nodes >= 2147483648.0) return false;
   return true;
 }
@@ -979,12 +983,17 @@ extern "C" {
 
 const char* hpc_last_error(void) { return g_err.c_str(); }
 
-int hpc_footprint(const hpc_geometry* geo, size_t* bytes) {
-  if (!geometry_ok(geo) || !bytes) return arg_fail("bad geometry");
+static int footprint(const hpc_geometry* geo, int nr, int r, size_t* bytes) {
+  if (!geometry_ok(geo, nr, r) || !bytes) return arg_fail("bad geometry");
   double box[6];
   HostLevel lv[kMaxLevels];
   host_geometry(*geo, box, lv);
+  SlabLevel sl[kMaxLevels];
+  slab_levels(*geo, nr, r, sl);
+  const int nz0 = lv[0].nz;  // the whole coarsest level (a split gathers it)
+  for (int l = 0; l <= geo->maxlevel; ++l) lv[l].nz = sl[l].nz;
   size_t total = 0;
+  if (nr > 1) total += sizeof(double) * 14 * (size_t)lv[0].px * lv[0].ny * nz0 + nz0;
   for (int l = 0; l <= geo->maxlevel; ++l) {
     long long n = (long long)lv[l].px * lv[l].ny * lv[l].nz;
     total += level_bytes(n) + (size_t)(lv[l].nx + lv[l].ny + lv[l].nz);
@@ -1006,13 +1015,20 @@ int hpc_footprint(const hpc_geometry* geo, size_t* bytes) {
   return HPC_OK;
 }
 
+int hpc_footprint(const hpc_geometry* geo, size_t* bytes) { return footprint(geo, 1, 0, bytes); }
+
+int hpc_footprint_slab(const hpc_geometry* geo, int nranks, int rank, size_t* bytes) {
+  if (nranks < 1 || rank < 0 || rank >= nranks) return arg_fail("bad slab rank");
+  return footprint(geo, nranks, rank, bytes);
+}
+
 static std::atomic<unsigned long long> g_ctx_uid{0};
 
 // hpc_create (a whole specimen) and hpc_create_slab (rank r of nr along z; `slab`).
 static int create_ctx(hpc_ctx** out, const hpc_geometry* geo, int device, int nr, int r, bool slab) {
   if (!out) return arg_fail("null output");
   *out = nullptr;
-  if (!geometry_ok(geo)) return arg_fail("bad geometry");
+  if (!geometry_ok(geo, nr, r)) return arg_fail("bad geometry");
   SlabLevel sl[kMaxLevels];
   if (!slab_levels(*geo, nr, r, sl)) return arg_fail("bad slab decomposition (every rank needs a coarsest plane)");
   int ndev = 0;

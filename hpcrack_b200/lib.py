@@ -121,6 +121,7 @@ SIGNATURES = {
     "hpc_dmax_noalloc": [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p],
     "hpc_slab_level": [C.POINTER(hpc_geometry), _i, _i, _i, _ip],
     "hpc_create_slab": [C.POINTER(C.c_void_p), C.POINTER(hpc_geometry), _i, _i, _i],
+    "hpc_footprint_slab": [C.POINTER(hpc_geometry), _i, _i, C.POINTER(C.c_size_t)],
     "hpc_slab_group_create": [C.POINTER(C.c_void_p), _i],
     "hpc_slab_group_join": [_vp, _ctx],
     "hpc_slab_group_abort": [_vp],

@@ -170,12 +170,17 @@ class Hierarchy:
         self.close()
 
     @staticmethod
-    def footprint(maxlevel, enb, x0=(0.0, 0.0, 0.0), roi=(0, 0, 0)) -> int:
+    def footprint(maxlevel, enb, x0=(0.0, 0.0, 0.0), roi=(0, 0, 0), slab=None) -> int:
+        """Device bytes of a context (hpc_footprint), or of one rank's slab: slab = (nranks, rank)."""
         lib = _L.load()
         geo = _L.hpc_geometry(int(maxlevel), (C.c_int * 3)(*map(int, enb)), (C.c_double * 3)(*map(float, x0)),
                               (C.c_int * 3)(*map(int, roi)))
         out = C.c_size_t(0)
-        _L.check("hpc_footprint", lib.hpc_footprint(C.byref(geo), C.byref(out)))
+        if slab is None:
+            _L.check("hpc_footprint", lib.hpc_footprint(C.byref(geo), C.byref(out)))
+        else:
+            _L.check("hpc_footprint_slab", lib.hpc_footprint_slab(C.byref(geo), int(slab[0]), int(slab[1]),
+                                                                  C.byref(out)))
         return out.value
 
     def _c(self, name, *args):

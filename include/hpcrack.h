@@ -377,8 +377,12 @@ int hpc_dmax_noalloc(const double* d, const double* d_old, long long n, double* 
  * past the last owned plane} of rank `rank` of `nranks` on `level`; HPC_ERR_ARG if a rank would own
  * no coarsest plane. */
 int hpc_slab_level(const hpc_geometry* geo, int nranks, int rank, int level, int* out4);
-/* A context for rank `rank` of `nranks`; it joins a transport before its first collective step. */
+/* A context for rank `rank` of `nranks`; it joins a transport before its first collective step.  The
+ * 2^31-node limit of hpc_create applies to each rank's planes, so a split specimen may exceed it (and
+ * one GPU's memory). */
 int hpc_create_slab(hpc_ctx** out, const hpc_geometry* geo, int device, int nranks, int rank);
+/* hpc_footprint of rank `rank`'s slab (its planes, and the whole coarsest level it gathers). */
+int hpc_footprint_slab(const hpc_geometry* geo, int nranks, int rank, size_t* bytes);
 /* In-process transport: the ranks are host threads of this process (each calling its own context,
  * all at once), on one device or several; planes move by device copies, reductions are combined
  * on the host in rank order (every rank gets the same bits).  A wait for a rank that does not

@@ -301,3 +301,26 @@ def test_slab_group_run_aborts_and_reraises_the_failing_rank():
     with pytest.raises(ValueError, match="rank 1 failed"):
         g.run(fn)
     assert g.run(lambda h: h.slab[1] * 10) == [0, 10, 20]
+
+
+def test_slab_footprints_let_a_specimen_exceed_one_gpu():
+    """hpc_footprint_slab: a rank holds its planes (plus the gathered coarsest level), so the split's
+    per-rank bytes shrink with the rank count.  1025^3 (every form's buffers: ~920 GB) fits 8 GPUs of
+    180 GB; 2049^3 (8.6e9 nodes) is past the 2^31-node limit of one context, refused whole and
+    accepted split over 64 ranks, each under 180 GB."""
+    from hpcrack_b200.solver import Hierarchy
+
+    whole = Hierarchy.footprint(5, (8, 8, 8))
+    assert Hierarchy.footprint(5, (8, 8, 8), slab=(1, 0)) == whole
+    for n in (2, 4, 8):
+        parts = [Hierarchy.footprint(5, (8, 8, 8), slab=(n, r)) for r in range(n)]
+        assert max(parts) < whole * (1.0 / n + 0.08), (n, max(parts), whole)
+        assert sum(parts) >= whole
+    big = Hierarchy.footprint(7, (8, 8, 8))
+    assert big > 180e9
+    assert all(Hierarchy.footprint(7, (8, 8, 8), slab=(8, r)) < 180e9 for r in range(8))
+    with pytest.raises(L.HpcError):  # 2049^3 as 64^3 coarsest elements: 64 ranks own a coarsest plane each
+        Hierarchy.footprint(5, (64, 64, 64))
+    assert all(Hierarchy.footprint(5, (64, 64, 64), slab=(64, r)) < 180e9 for r in (0, 1, 63))
+    with pytest.raises(L.HpcError):  # 9 coarsest planes cannot go to 10 ranks (initialization.cpp:50-72)
+        Hierarchy.footprint(5, (8, 8, 8), slab=(10, 0))
