@@ -200,3 +200,36 @@ def test_slab_refusals_and_abort():
         assert time.time() - t0 < 60
     finally:
         split.close()
+
+
+def test_split_cracked_specimen_matches_the_oracle():
+    """crack33 (the benchmarked recipe: pores, inclusions, pre-crack) split over 3 ranks against the C
+    oracle, which the reference's own goldens pin: the first increment within 1e-10 on u, d, H with
+    equal V-cycle and finest-iteration counts, the second within the reference's own run-to-run
+    spread on u and the reaction (tests/cases.py), d and H within 1e-10."""
+    from oracle.bindings import COracle
+
+    w = ms.make_workload("crack33")
+    split = SlabGroup(w.maxlevel, w.element_nb, 3, x0=w.x_start)
+    orc = COracle(w.maxlevel, w.element_nb, x0=w.x_start)
+    try:
+        load_workload([split, orc], w)
+        Lf = w.maxlevel
+        kw = dict(ut0=w.ut0, dU=w.du, mech_tol=w.mech_tol, pf_tol=w.pf_tol)
+        for t in range(2):
+            og = split.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, **kw)
+            oo = orc.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, **kw)
+            assert og[5] == oo[5] and og[7] == oo[7], (t, og, oo)
+            if t == 0:
+                assert og[4] == oo[4] and og[6] == oo[6], (t, og, oo)
+                assert rel(split.get(U, Lf), orc.get(U, Lf)) < 1e-10
+                assert abs(og[1] - oo[1]) <= 1e-10 * abs(oo[1])
+            else:
+                assert abs(og[4] - oo[4]) <= CRACK_CYCLE_SLACK, (t, og, oo)
+                assert rel(split.get(U, Lf), orc.get(U, Lf)) < CRACK_U_TOL[w.mech_tol], t
+                assert abs(og[1] - oo[1]) <= CRACK_F_TOL[w.mech_tol] * abs(oo[1]), t
+            assert rel(split.get(D, Lf), orc.get(D, Lf)) < 1e-10, t
+            assert rel(split.get(H, Lf), orc.get(H, Lf)) < 1e-10, t
+    finally:
+        split.close()
+        orc.close()
