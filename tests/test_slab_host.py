@@ -324,3 +324,23 @@ def test_slab_footprints_let_a_specimen_exceed_one_gpu():
     assert all(Hierarchy.footprint(5, (64, 64, 64), slab=(64, r)) < 180e9 for r in (0, 1, 63))
     with pytest.raises(L.HpcError):  # 9 coarsest planes cannot go to 10 ranks (initialization.cpp:50-72)
         Hierarchy.footprint(5, (8, 8, 8), slab=(10, 0))
+
+
+def test_slab_group_lifecycle_without_a_device():
+    """The in-process group is host state: create, refuse bad joins, abort, destroy - no device needed."""
+    import ctypes as C
+
+    lib = L.load()
+    g = C.c_void_p()
+    assert lib.hpc_slab_group_create(C.byref(g), 0) == 1          # HPC_ERR_ARG: no ranks
+    assert lib.hpc_slab_group_create(C.byref(g), 65) == 1         # beyond the group's rank table
+    assert lib.hpc_slab_group_create(C.byref(g), 3) == 0
+    assert lib.hpc_slab_group_join(g, None) == 1                  # no context
+    assert lib.hpc_slab_group_join(None, None) == 1
+    assert lib.hpc_slab_group_abort(g) == 0
+    assert lib.hpc_slab_group_abort(None) == 1
+    assert lib.hpc_slab_group_destroy(g) == 0
+    assert lib.hpc_slab_group_destroy(None) == 0
+    assert lib.hpc_slab_join_nccl(None, None) == 1
+    out = (C.c_int * 4)()
+    assert lib.hpc_slab_level(None, 2, 0, 0, out) == 1
