@@ -67,6 +67,11 @@ def parse_args():
     ap.add_argument("--no-tma", action="store_true",
                     help="stage the finest applies' node rows with per-lane cp.async instead of tensor copies "
                          "(hpc_set_tma_staging 0)")
+    ap.add_argument("--cpu-plan-runs", default="parity65:3,crack65:2,parity129:3", metavar="NAME:K[,...]",
+                    help="--cpu-plan: the workloads and increment counts of its full runs")
+    ap.add_argument("--cpu-plan-gpu-only", action="store_true",
+                    help="--cpu-plan: only the B200 side of the full runs (the reference's side: "
+                         "python -m oracle.time_reference NAME K)")
     ap.add_argument("--split", choices=("replicas", "slab"), default="replicas",
                     help="replicas: one specimen per GPU (weak scaling, the default); slab: one specimen split "
                          "along z over the GPUs, one rank each over NCCL (strong scaling)")
@@ -822,7 +827,7 @@ def run_cpu_plan(args, local):
             ref.voigt_all_level(H)
         return ref, t_in
 
-    for name in ("crack65", "mid129", "plain257"):
+    for name in (() if args.cpu_plan_gpu_only else ("crack65", "mid129", "plain257")):
         w = ms.make_workload(name)
         L = w.maxlevel
         gpu = load_specimen(w, local)
@@ -857,18 +862,20 @@ def run_cpu_plan(args, local):
         gpu.close()
         print(json.dumps(out["applies"][-1]), flush=True)
 
-    for name, steps in (("parity65", 3), ("crack65", 2)):
+    runs = [(r.split(":")[0], int(r.split(":")[1])) for r in args.cpu_plan_runs.split(",") if r]
+    for name, steps in runs:
         w = ms.make_workload(name)
         L = w.maxlevel
-        ref, _ = ref_for(w)
+        ref = None if args.cpu_plan_gpu_only else ref_for(w)[0]
         gpu = load_specimen(w, local)
         rec = {"workload": name, "increments": steps, "tolerance": "the reference's own: |r|^2/|f|^2 <= 1e-6, "
                                                                     "|R|^2/|fd|^2 <= 1e-12", "cpu": [], "gpu": []}
         for t in range(steps):
-            t0 = time.perf_counter()
-            o = ref.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du)
-            rec["cpu"].append({"t": t, "s": time.perf_counter() - t0, "mech_cycles": int(o[4]), "pf_cycles": int(o[5]),
-                               "mech_iters": int(o[6]), "pf_iters": int(o[7])})
+            if ref is not None:
+                t0 = time.perf_counter()
+                o = ref.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du)
+                rec["cpu"].append({"t": t, "s": time.perf_counter() - t0, "mech_cycles": int(o[4]),
+                                   "pf_cycles": int(o[5]), "mech_iters": int(o[6]), "pf_iters": int(o[7])})
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             og = gpu.step(t, w.mg_u, w.mg_d, w.small_k, w.lc, w.voxel_size, ut0=w.ut0, dU=w.du)
@@ -876,14 +883,15 @@ def run_cpu_plan(args, local):
                                "pf_cycles": int(og[5])})
         nx, ny, nz = w.nodes
         n = nx * ny * nz
-        ct = sum(r["s"] for r in rec["cpu"])
-        cit = sum(3.0 * n * r["mech_iters"] + n * r["pf_iters"] for r in rec["cpu"])
-        rec["cpu_mdof_iter_per_s"] = cit / ct / 1e6
-        rec["cpu_s_per_v_cycle"] = ct / max(1, sum(r["mech_cycles"] + r["pf_cycles"] for r in rec["cpu"]))
+        if ref is not None:
+            ct = sum(r["s"] for r in rec["cpu"])
+            cit = sum(3.0 * n * r["mech_iters"] + n * r["pf_iters"] for r in rec["cpu"])
+            rec["cpu_mdof_iter_per_s"] = cit / ct / 1e6
+            rec["cpu_s_per_v_cycle"] = ct / max(1, sum(r["mech_cycles"] + r["pf_cycles"] for r in rec["cpu"]))
+            rec["cpu_s"] = ct
+            ref.close()
         rec["gpu_s"] = sum(r["s"] for r in rec["gpu"])
-        rec["cpu_s"] = ct
         out["runs"].append(rec)
-        ref.close()
         gpu.close()
         print(json.dumps(rec), flush=True)
     print(json.dumps(out), flush=True)

@@ -196,10 +196,11 @@ def make_workload(name: str) -> Workload:
     * ``crack33`` / ``crack65``  the plain257 recipe (three phases, pre-crack) scaled to 33^3 / 65^3,
       the parity cases of the benchmarked configuration (the reference finishes them in minutes).
     * ``large513``  513^3, seed 2, inclusions to 30 %.
-    * ``small17`` / ``small33`` test-sized variants of parity65.
+    * ``small17`` / ``small33`` test-sized variants of parity65; ``parity129`` the same recipe at 129^3
+      (the CPU baseline's second full-run size).
     """
-    if name in ("parity65", "small17", "small33"):
-        n = {"parity65": 65, "small17": 17, "small33": 33}[name]
+    if name in ("parity65", "parity129", "small17", "small33"):
+        n = {"parity65": 65, "parity129": 129, "small17": 17, "small33": 33}[name]
         scale = (n - 1) / 64.0
         img = sphere_image((n, n, n), 0, [Phase(INCLUSION_GRAY, 4 * scale, 8 * scale, count=12)])
         return Workload(name, img, (8, 8, 8), maxlevel_for(n, 0, 8), (0.0, 0.0, 0.0), 1e-6, 2.0, 1e-6,
